@@ -1,0 +1,373 @@
+"""Benchmark of the fused two-phase jet step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 128 x 128 x 512 D3Q27 + D3Q7 oil jet (nozzle diameter 16,
+w = 0.05 with 1 % Gaussian inlet noise, seed 1, tau = 0.52, sigma = 1e-3,
+interface width 4, mobility 0.1, exact periodic x and y, inflow at z = 0 and
+outflow at z = nz-1), FP32 population storage.  Synthetic input: the jet
+starts from quiescent water, the reference's own initial state.  A step is one
+time step of the whole lattice (bulk kernel + boundary kernels, as a CUDA graph
+of 2 steps replayed).  MLUPS counts all nx*ny*nz cells per step, the
+reference's convention (src/main.cu:199-203).
+
+Multi-GPU: the workload does not shard (one lattice per GPU); with --gpus N
+every rank runs an independent replica ("weak" scaling, no collective in the
+data path) and rank 0 reports the sum of MLUPS over ranks timed as the max
+device time over ranks.
+
+--impl reference runs the reference's own CUDA kernels for the same
+configuration (its only implementation of the path), built from its sources
+by ``python -m oracle.build --ref`` into oracle/_ref/q27_c2/harness, on the
+same GPU with the reference's own step loop (graph + boundary launches +
+per-step stream synchronisation, src/main.cu:159-172).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 128, 128, 512
+Q = 27
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def b_alg(q: int, s_f: int) -> int:
+    """Compulsory bytes per cell update: read + write of f (q s_f), g (7 s_f) and phi (4)."""
+    return 2 * (q * s_f + 7 * s_f + 4)
+
+
+def hbm_peak():
+    try:
+        d = json.load(open(PEAKS_FILE))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms while active."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            c = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(c[1]))
+                smax = float(c[2])
+                power.append(float(c[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "power_w_max": max(power) if power else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def workload(storage: int, q: int = Q):
+    from ssmdlbm_b200 import configs
+    return configs.oil_jet(NX, NY, NZ, q, tau=0.52, sigma=1e-3, width=4.0, mobility=0.1, diam=16,
+                           w_in=0.05, noise=0.01, seed=1, storage=storage)
+
+
+def time_graph(sim, steps: int, warmup: int, world: int):
+    """Device time of `steps` steps replayed as 2-step graphs (max over ranks)."""
+    import torch
+    sim.graph(2)
+    sim.run_graph(max(1, warmup // 2), 2)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    s = sim.torch_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    sim.run_graph(steps // 2, 2)
+    e1.record(s)
+    e1.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    return max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+
+
+def bulk_launch_ms(sim, launches: int) -> float:
+    """Mean duration of the fused bulk kernel, CUDA events on its stream."""
+    from ssmdlbm_b200 import _lib
+    L = _lib.lib()
+    _lib.check(L.ssmd_profile_enable(launches))
+    sim.step(launches)
+    ms = (ctypes.c_float * launches)()
+    cnt = ctypes.c_int32()
+    _lib.check(L.ssmd_profile_read(ms, launches, ctypes.byref(cnt)))
+    _lib.check(L.ssmd_profile_disable())
+    vals = list(ms)[:cnt.value]
+    return statistics.mean(vals)
+
+
+def e2e_run(p, steps: int):
+    """End to end through the C ABI with host buffers: pinned upload of the
+    initial macroscopic state, ssmd_init_from_macros, `steps` calls of
+    ssmd_step each followed by an async read-back of the status word, and the
+    download of phi and rho (the fields the reference's pipeline saves)."""
+    import numpy as np
+    import torch
+    from ssmdlbm_b200 import _lib
+    from ssmdlbm_b200.lbm import Simulation
+    sim = Simulation(p)
+    n = sim.cells
+    sim.init()  # the reference's initial state, staged in pinned host memory (untimed)
+    sim.sync()
+    host_in = {k: torch.empty(n, dtype=torch.float32, pin_memory=True) for k in ("rho", "ux", "uy", "uz", "phi")}
+    for k, t in host_in.items():
+        t.copy_(sim.t[k])
+    host_out = {k: torch.empty(n, dtype=torch.float32, pin_memory=True) for k in ("phi", "rho")}
+    status_host = torch.empty(4, dtype=torch.uint8, pin_memory=True)
+    L = _lib.lib()
+    s = sim.torch_stream
+    pr, fl = ctypes.byref(sim.p), ctypes.byref(sim.fields)
+
+    def once(k):
+        with torch.cuda.stream(s):
+            for name, t in host_in.items():
+                sim.t[name].copy_(t, non_blocking=True)
+            _lib.check(L.ssmd_init_from_macros(pr, fl, sim.stream))
+            for i in range(k):
+                flags = _lib.STEP_STORE_MACROS if i == k - 1 else 0
+                _lib.check(L.ssmd_step(fl, pr, i, flags, sim.stream))
+                status_host.copy_(sim.t["workspace"][:4], non_blocking=True)
+            for name, t in host_out.items():
+                t.copy_(sim.t[name], non_blocking=True)
+        s.synchronize()
+
+    once(4)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    once(steps)
+    dt = time.perf_counter() - t0
+    h2d = 5 * n * 4 / steps
+    d2h = (2 * n * 4) / steps + 4
+    sim.close()
+    return n * steps / dt / 1e6, h2d, d2h
+
+
+def cpu_baseline(p, steps: int = 3):
+    """FP64 oracle (the CPU restatement of the step) on the host cores."""
+    from oracle.oracle import Oracle
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    o = Oracle(p, 64)
+    o.init_jets()
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    n = int(p.nx) * int(p.ny) * int(p.nz)
+    return {"value": n * steps / dt / 1e6, "unit": "MLUPS", "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "kind": "port",
+            "sample": f"FP64 oracle, {steps} steps of the full {NX}x{NY}x{NZ} D3Q27+D3Q7 lattice after 1 "
+                      f"warm-up step ({dt:.1f} s)"}
+
+
+def run_ours(a, world, rank, local):
+    import torch
+    from ssmdlbm_b200 import _lib
+    from ssmdlbm_b200.lbm import Simulation
+
+    p = workload(_lib.STORAGE_F32)
+    sim = Simulation(p)
+    sim.init()
+    with ClockSampler(local) as clk:
+        dt = time_graph(sim, a.steps, a.warmup, world)
+    clocks = clk.summary()
+    mlups_rank = sim.cells * a.steps / dt / 1e6
+    value = mlups_rank * world
+    st = sim.reduce(raise_unstable=False)
+
+    # live roofline of the dominant kernel
+    bulk_ms = bulk_launch_ms(sim, 40)
+    bytes_per_launch = b_alg(Q, 4) * sim.cells
+    peak, peak_kind = hbm_peak()
+    achieved = bytes_per_launch / (bulk_ms * 1e-3) / 1e9
+    n_bc = 2 + 0  # oil inflow + outflow z (x, y exact periodic: no ghost copies)
+    sim.close()
+    del sim
+    torch.cuda.empty_cache()
+
+    variants = {}
+    if not a.quick:
+        for name, q, stg in (("d3q27_f16", 27, _lib.STORAGE_F16), ("d3q27_bf16", 27, _lib.STORAGE_BF16),
+                             ("d3q19_f32", 19, _lib.STORAGE_F32), ("d3q19_f16", 19, _lib.STORAGE_F16)):
+            pv = workload(stg, q)
+            sv = Simulation(pv)
+            sv.init()
+            dv = time_graph(sv, a.steps, a.warmup, world)
+            bm = bulk_launch_ms(sv, 20)
+            s_f = 4 if stg == _lib.STORAGE_F32 else 2
+            variants[name] = {"mlups": round(sv.cells * a.steps / dv / 1e6, 1),
+                              "bulk_ms": round(bm, 4),
+                              "roofline_frac": round(b_alg(q, s_f) * sv.cells / (bm * 1e-3) / 1e9 / peak, 4)}
+            sv.close()
+            del sv
+            torch.cuda.empty_cache()
+
+    e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
+    e2e_mlups = e2e_mlups * world
+
+    line = {
+        "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt * 1e3 / a.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: quiescent water + noisy oil inlet (the reference's initial state)",
+        "config": {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, FP32 storage, nozzle 16, tau 0.52, "
+                               "w 0.05 + 1% noise, seed 1",
+                   "cells": NX * NY * NZ, "velocity_set": "D3Q27", "storage": "f32",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (populations 0.9 GB per buffer)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "kernel": "ssmd::bulk_kernel<27,float,float>",
+                     "bytes_per_cell": b_alg(Q, 4), "launch_ms": round(bulk_ms, 4)},
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": a.steps * (1 + n_bc),
+        "clocks": clocks,
+        "variants": variants,
+        "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
+    }
+    if rank == 0 and world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(workload(_lib.STORAGE_F32), steps=3)
+    return line
+
+
+def run_reference(a, world, rank):
+    if rank != 0:
+        return None
+    sys.path.insert(0, ROOT)
+    from oracle import build as obuild
+    exe = obuild.ref_binary("q27_c2")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": f"reference harness not built ({exe})"}
+    # the reference cannot express inlet noise, the centred nozzle, exact periodic
+    # faces or M = 0.1; its closest run: same lattice, velocity sets, tau, sigma,
+    # nozzle diameter and inlet speed, its own boundary set with y copy-periodic.
+    out = subprocess.run([exe, "--periodic-y", "--time", f"{a.warmup},{a.steps}"], capture_output=True,
+                         text=True, timeout=1200, check=True).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    v = r["mlups"]
+    return {
+        "metric": "MLUPS", "value": round(v, 1), "unit": "MLUPS", "n_gpus": 1, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "data": "synthetic: the reference's own initial state",
+        "config": {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, FP32 storage, nozzle 16, tau 0.52 "
+                               "(reference build: no noise, nozzle at (nx-1)/2, (ny-1)/4, M = 0.125)",
+                   "cells": NX * NY * NZ, "velocity_set": "D3Q27", "storage": "f32",
+                   "parallelism": "single GPU"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "MLUPS", "cores": 1, "kind": "reference",
+                         "sample": "the reference's own CUDA kernels (its only implementation of the "
+                                   "path), built for sm_100a from its sources, driven by one host "
+                                   "thread with its per-step stream synchronisation"},
+        "e2e": {"value": round(v, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--quick", action="store_true", help="skip the storage / velocity-set variants")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    a = ap.parse_args()
+    if a.steps % 2:
+        a.steps += 1
+    a.warmup = max(a.warmup, 4)
+    world, rank, local = dist_setup(a.gpus)
+    if a.impl == "reference":
+        line = run_reference(a, world, rank)
+    else:
+        line = run_ours(a, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

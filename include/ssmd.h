@@ -1,0 +1,276 @@
+/*
+ * ssmd.h — C ABI of the B200 (sm_100a) two-phase jet lattice-Boltzmann step.
+ *
+ * One time step of the reference (ssmdLBM) is the CUDA graph
+ *   computePhase -> computeForces -> computeMoments -> streamCollide
+ * (src/cuda/CUDAGraph.cuh:41-56) followed by five boundary launches
+ * (src/main.cu:165-169).  This library replaces that sequence with one fused
+ * bulk kernel plus light surface kernels, behind the entry points below.
+ *
+ * Conventions shared by every entry point
+ *   - All pointers inside LBMFields and ssmd_params are DEVICE pointers that
+ *     the caller owns (cudaMalloc, a caching allocator, ...).  No entry point
+ *     allocates or frees device memory.
+ *   - Every call is asynchronous on the given stream unless it says it
+ *     synchronises.  Return value: 0 (SSMD_OK) or a positive SSMD_ERR_* code;
+ *     ssmd_last_error() returns a message for the calling thread.  The library
+ *     never aborts the process (the reference's checkCudaErrors* macros do,
+ *     src/cuda/utils.cuh:101-161; that policy stays with the caller).
+ *   - Scalar fields are FP32, structure of arrays, index x + nx*(y + ny*z)
+ *     (reference src/functions/deviceFunctions.cuh:33-39).  Populations are
+ *     [q][cell] arrays with q in the reference's velocity order
+ *     (src/velocitySet/D3Q19.cuh:82-131, D3Q27.cuh:91-140, D3Q7.cuh:73-122),
+ *     stored in PULL layout: slot q of cell s holds the post-collision value
+ *     that cell s + c_q reads next step.  ssmd_populations_to_push() converts
+ *     to the reference's post-stream (push) layout.  Cell indices are 32-bit,
+ *     population offsets 64-bit, so nx*ny*nz may reach 2^32 - 1 cells.
+ *   - One host thread per stream.  Graph capture of ssmd_step is legal on the
+ *     caller's stream (no host synchronisation inside a step).
+ */
+#ifndef SSMD_H
+#define SSMD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque CUDA handles, layout-identical to cudaStream_t / cudaGraphExec_t. */
+typedef struct CUstream_st *ssmd_stream_t;
+typedef struct CUgraphExec_st *ssmd_graph_exec_t;
+
+#define SSMD_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+#define SSMD_OK 0
+#define SSMD_ERR_INVALID_ARGUMENT 1 /* bad size, pointer or parameter      */
+#define SSMD_ERR_CUDA 2             /* a CUDA runtime call failed          */
+#define SSMD_ERR_UNSTABLE 3         /* NaN/Inf or |u| above the limit       */
+#define SSMD_ERR_UNSUPPORTED 4      /* combination not built into library  */
+
+/* ------------------------------------------------------ face-pair kinds */
+#define SSMD_BC_PERIODIC_COPY 0 /* reference periodicX: ghost layers at 0 and n-1,
+                                   slots copied between planes 1 and n-2
+                                   (src/BoundaryConditions.cuh:295-349)       */
+#define SSMD_BC_PERIODIC 1      /* exact periodic wrap, no ghost layers       */
+#define SSMD_BC_JET 2           /* y: water inflow disc at y=0 + outflow at
+                                   y=ny-1 (BoundaryConditions.cuh:36-99,170-233);
+                                   z: oil inflow disc at z=0 + outflow at
+                                   z=nz-1 (:101-168, :235-293)                 */
+
+/* ------------------------------------------------------- storage types */
+#define SSMD_STORAGE_F32 0  /* f - w_q and g as float                        */
+#define SSMD_STORAGE_F16 1  /* f - w_q and g as IEEE half (round to nearest) */
+#define SSMD_STORAGE_BF16 2 /* f - w_q and g as bfloat16 (round to nearest)  */
+
+/* ------------------------------------------------------------ step flags */
+#define SSMD_STEP_STORE_MACROS 1u /* write rho, ux, uy, uz, phi at every cell */
+
+/*
+ * Field container.  Member order and meaning are those of the reference's
+ * struct LBMFields (src/structs/LBMFields.cuh:26-49) so code that reads
+ * fields.phi / fields.rho after a step keeps working.  f and g point at the
+ * "A" population buffers; the "B" buffers are ssmd_params.f_alt / g_alt.
+ * normx/normy/normz/ind are never used (the reference never allocates them
+ * either, src/main.cu:55-70).
+ */
+typedef struct LBMFields {
+    float *rho;
+    float *ux;
+    float *uy;
+    float *uz;
+    float *pxx;
+    float *pyy;
+    float *pzz;
+    float *pxy;
+    float *pxz;
+    float *pyz;
+    float *phi;
+    float *normx;
+    float *normy;
+    float *normz;
+    float *ind;
+    float *fsx;
+    float *fsy;
+    float *fsz;
+    void *f; /* Q * cells populations, element type from ssmd_params.storage */
+    void *g; /* 7 * cells phase populations, same element type              */
+} LBMFields;
+
+/*
+ * Run-time parameters.  The reference fixes all of these at compile time
+ * (src/constants.cuh:70-101, src/functions/globalFunctions.cuh:68-104,
+ * 232-283); here they are per call so one library serves every grid.
+ * Floating-point members are the FP32 values the kernels use, so a caller can
+ * reproduce the reference's constexpr arithmetic bit for bit
+ * (ssmd_params_reference does exactly that).
+ */
+typedef struct ssmd_params {
+    uint32_t nx, ny, nz;  /* lattice size, ghost layers included              */
+    int32_t velocity_set; /* 19 or 27 (hydrodynamics); phase field is D3Q7    */
+    int32_t storage;      /* SSMD_STORAGE_*                                   */
+    int32_t bc_x;         /* SSMD_BC_PERIODIC_COPY | SSMD_BC_PERIODIC          */
+    int32_t bc_y;         /* SSMD_BC_PERIODIC_COPY | SSMD_BC_PERIODIC | SSMD_BC_JET */
+    int32_t bc_z;         /* SSMD_BC_JET | SSMD_BC_PERIODIC                    */
+
+    float nu_water;   /* kinematic viscosity of phi = 0 (lattice units)       */
+    float nu_oil;     /* kinematic viscosity of phi = 1                       */
+    float omco_water; /* 1 - omega(nu_water), water inflow regularisation     */
+    float omco_oil;   /* 1 - omega(nu_oil), oil inflow regularisation         */
+    float omco_ref;   /* 1 - omega used by the outflows (reference: water)    */
+    float sigma;      /* surface tension                                      */
+    float gamma;      /* interface sharpening 4 M / (W cs2)                   */
+    float omega_g;    /* phase-field BGK rate 1/(1/2 + M/cs2); 1 = reference  */
+
+    float u_oil;     /* oil inlet speed (+z) at z = 0                        */
+    float oil_cx;    /* oil disc centre x                                    */
+    float oil_cy;    /* oil disc centre y                                    */
+    float oil_r2;    /* oil disc radius squared (cells with r^2 <= oil_r2)   */
+    float u_water;   /* water inlet speed (+y) at y = 0                      */
+    float water_cx;  /* water disc centre x                                  */
+    float water_cz;  /* water disc centre z                                  */
+    float water_r2;  /* water disc radius squared                            */
+    float noise_amp; /* oil inlet speed u_oil * (1 + noise_amp * N(0,1))     */
+    float u_limit;   /* |u| above this is reported as SSMD_ERR_UNSTABLE      */
+    uint64_t seed;   /* key of the counter-based inlet noise                 */
+
+    void *f_alt;      /* "B" hydrodynamic populations, same size as fields->f */
+    void *g_alt;      /* "B" phase populations, same size as fields->g        */
+    void *workspace;  /* ssmd_workspace_bytes() bytes of device scratch       */
+    size_t workspace_bytes;
+
+    int32_t tile_z;   /* z planes per bulk work item (0: library default)     */
+    int32_t reserved[7];
+} ssmd_params;
+
+/* Global reductions, accumulated in FP64 over the fluid (non-ghost) cells. */
+typedef struct ssmd_stats {
+    double phi_sum;      /* sum of phi from the macroscopic field             */
+    double phi_sum_next; /* sum over cells of sum_q g (next step's phi)        */
+    double mass;         /* sum of rho                                        */
+    double momentum[3];  /* sum of rho u                                      */
+    double kinetic;      /* sum of rho |u|^2 / 2                              */
+    double u_max;        /* max |u|                                           */
+    double nonfinite;    /* count of cells with non-finite rho, u or phi      */
+    double cells;        /* number of fluid cells reduced                     */
+} ssmd_stats;
+
+/* -------------------------------------------------------------- queries */
+int ssmd_abi_version(void);
+const char *ssmd_last_error(void);
+
+/* Bytes of one scalar field, of fields->f (== f_alt), of fields->g
+ * (== g_alt) and of the workspace, for these parameters. */
+size_t ssmd_scalar_bytes(const ssmd_params *p);
+size_t ssmd_f_bytes(const ssmd_params *p);
+size_t ssmd_g_bytes(const ssmd_params *p);
+size_t ssmd_workspace_bytes(const ssmd_params *p);
+
+/* Checks sizes, BC kinds, relaxation ranges (tau > 1/2) and geometry. */
+int ssmd_validate(const ssmd_params *p);
+
+/*
+ * Fills p the way the reference derives its constants:
+ *   nu = u * diam / Re (FP64 then FP32, globalFunctions.cuh:234-242),
+ *   omega = 1/(1/2 + 3 nu) in FP64 (:244-247), omco = 1 - omega (:269-282),
+ *   sigma = u_oil^2 diam_oil / We (constants.cuh:93),
+ *   gamma = 4 cs2 (tau_g - 1/2) / W / cs2 with tau_g = 1 (constants.cuh:97-100),
+ *   disc radius = diam / 2 in integers, r^2 = radius^2 (globalFunctions.cuh:70-78),
+ *   oil centre ((nx-1)/2, (ny-1)/4), water centre ((nx-1)/2, 0.35 (nz-1)).
+ * Boundary kinds default to the reference's two-jet crossflow:
+ * bc_x = PERIODIC_COPY, bc_y = JET, bc_z = JET.
+ * radius_* may be passed separately from diam_* (radius < 0: diam / 2).
+ */
+int ssmd_params_reference(ssmd_params *p, uint32_t nx, uint32_t ny, uint32_t nz,
+                          int32_t velocity_set, float u_water, float u_oil,
+                          int32_t diam_water, int32_t diam_oil, int32_t radius_water,
+                          int32_t radius_oil, double reynolds_water, double reynolds_oil,
+                          double weber, float interface_width);
+
+/* ------------------------------------------------------------- the path */
+
+/*
+ * Initial state of the reference (src/initialConditions.cu:33-140):
+ * rho = 1, u = 0, phi = 0; phi = 0, uy = u_water on the water disc (bc_y = JET);
+ * phi = 1, uz = u_oil on the oil disc (bc_z = JET); f = f_eq(rho, u) and
+ * g = g_eq(phi, u) in both population buffers.  Zeroes pxx..pyz and fsx..fsz.
+ * Resets the device step counter to 0.
+ */
+int ssmd_init(const ssmd_params *p, LBMFields *fields, ssmd_stream_t stream);
+
+/*
+ * Same, but takes rho, ux, uy, uz and phi as the caller left them in fields
+ * (the reference's setDistros on an arbitrary macroscopic state,
+ * initialConditions.cu:99-140).
+ */
+int ssmd_init_from_macros(const ssmd_params *p, LBMFields *fields, ssmd_stream_t stream);
+
+/*
+ * One time step n = step: reads populations from the A buffers (fields->f/g)
+ * when step is even, from the B buffers (p->f_alt/g_alt) when odd, writes the
+ * other pair.  After the call, rho/u/Pi/phi are valid on the planes the
+ * boundaries read, phi/rho/u on the boundary faces, and, with
+ * SSMD_STEP_STORE_MACROS, rho/ux/uy/uz/phi on every cell (phi is the
+ * step-n field Sum_q g^n, as in the reference).
+ */
+int ssmd_step(LBMFields *fields, const ssmd_params *p, uint64_t step, uint32_t flags,
+              ssmd_stream_t stream);
+
+/*
+ * Captures steps [first_step, first_step + steps) into a CUDA graph and
+ * instantiates it (graph::captureGraph, src/cuda/CUDAGraph.cuh:34-57, which
+ * holds only the four bulk kernels; here the boundaries are inside too).
+ * steps must be even so that replays keep the A/B parity.  The inlet-noise
+ * step index lives in device memory and advances on every replayed step.
+ */
+int ssmd_capture_graph(const ssmd_params *p, LBMFields *fields, uint64_t first_step,
+                       int32_t steps, uint32_t flags, ssmd_stream_t stream,
+                       ssmd_graph_exec_t *out);
+
+/* Replays / frees a graph from ssmd_capture_graph (cudaGraphLaunch /
+ * cudaGraphExecDestroy through this library's runtime). */
+int ssmd_graph_launch(ssmd_graph_exec_t exec, ssmd_stream_t stream);
+int ssmd_graph_destroy(ssmd_graph_exec_t exec);
+
+/*
+ * FP64 reductions over the fluid cells (synchronises the stream).  Reads the
+ * macroscopic arrays (valid after a step with SSMD_STEP_STORE_MACROS or after
+ * init) and the current phase populations of step `steps_done` (number of
+ * steps taken since init).  Returns SSMD_ERR_UNSTABLE (with *out filled) when
+ * a non-finite value or |u| > p->u_limit is found.
+ */
+int ssmd_reduce(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done,
+                ssmd_stats *out, ssmd_stream_t stream);
+
+/*
+ * Copies the current populations (after `steps_done` steps) to the
+ * reference's push layout: which = 0 -> hydrodynamic f (element type of the
+ * storage), which = 1 -> g.  out has ssmd_f_bytes / ssmd_g_bytes bytes.
+ * Slots whose pull home lies outside the lattice are written as zero.
+ */
+int ssmd_populations_to_push(const ssmd_params *p, const LBMFields *fields,
+                             uint64_t steps_done, int32_t which, void *out,
+                             ssmd_stream_t stream);
+
+/*
+ * Kernel timing for benchmarks (host-side state of the calling thread, no
+ * device allocation): after ssmd_profile_enable(n), the next n ssmd_step
+ * calls record a CUDA event pair around their bulk-kernel launch;
+ * ssmd_profile_read synchronises and returns the launch durations in ms
+ * (count = recorded launches); ssmd_profile_disable frees the events.
+ */
+int ssmd_profile_enable(int32_t max_launches);
+int ssmd_profile_read(float *ms, int32_t max, int32_t *count);
+int ssmd_profile_disable(void);
+
+/* Reads and clears the device status word (synchronises the stream):
+ * bit 0 = a bulk cell produced a non-finite density. */
+int ssmd_check_status(const ssmd_params *p, uint32_t *status_out, ssmd_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSMD_H */

@@ -1,0 +1,121 @@
+// common.cuh — storage types, kernel arguments and lattice indexing.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "lattice.cuh"
+
+namespace ssmd {
+
+// ------------------------------------------------------------- storage
+// Populations are kept "shifted" (f - w_q, reference src/cuda/utils.cuh:67-99);
+// the reduced types only change the element type, arithmetic stays FP32.
+template <class T>
+struct Store;
+
+template <>
+struct Store<float> {
+    static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
+    static __device__ __forceinline__ float ldc(const float *p) { return *p; } // coherent (same-kernel writers)
+    static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
+};
+template <>
+struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+    static __device__ __forceinline__ float ldc(const __half *p) { return __half2float(*p); }
+    static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
+};
+template <>
+struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) {
+        return __bfloat162float(__ldg(p));
+    }
+    static __device__ __forceinline__ float ldc(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+// ------------------------------------------------------------- arguments
+enum : int { BC_COPY = 0, BC_PERIODIC = 1, BC_JET = 2 };
+
+struct DeviceStatus {
+    unsigned int flags;      // bit 0: non-finite density seen in the bulk
+    unsigned int pad0;
+    unsigned long long step; // index of the step in progress (inlet noise)
+    unsigned int work_next;  // persistent-kernel work counter
+    unsigned int pad1[11];
+};
+
+struct Geometry {
+    uint32_t nx, ny, nz;
+    uint32_t nxy;   // nx * ny
+    uint64_t cells; // nx * ny * nz
+    int bcx, bcy, bcz;
+    // fluid (colliding) index range per axis: [lo, hi]
+    int x_lo, x_hi, y_lo, y_hi, z_lo, z_hi;
+};
+
+struct Physics {
+    float nu_water, nu_oil_minus_water;
+    float omco_water, omco_oil, omco_ref;
+    float sigma, gamma, omega_g;
+    float u_oil, oil_cx, oil_cy, oil_r2;
+    float u_water, water_cx, water_cz, water_r2;
+    float noise_amp;
+    unsigned long long seed;
+};
+
+struct Fields {
+    float *rho, *ux, *uy, *uz;
+    float *pxx, *pyy, *pzz, *pxy, *pxz, *pyz;
+    float *phi;
+};
+
+template <class TF, class TG>
+struct StepArgs {
+    Geometry geo;
+    Physics phys;
+    Fields fld;
+    const TF *__restrict__ f_src;
+    TF *__restrict__ f_dst;
+    const TG *__restrict__ g_src;
+    TG *__restrict__ g_dst;
+    DeviceStatus *status;
+    uint32_t flags;       // SSMD_STEP_*
+    int tiles_x, tiles_y; // bulk tiling
+    int zchunk, nzchunks;
+};
+
+// ------------------------------------------------------------- indexing
+__host__ __device__ __forceinline__ uint32_t cell_index(const Geometry &g, uint32_t x, uint32_t y,
+                                                        uint32_t z) {
+    return x + g.nx * y + g.nxy * z;
+}
+
+__host__ __device__ __forceinline__ uint64_t slot(const Geometry &g, int q, uint32_t idx) {
+    return (uint64_t)q * g.cells + idx;
+}
+
+// Neighbour coordinate along one axis, with wrap when the axis is periodic.
+// Returns -1 when the coordinate leaves a non-periodic lattice.
+__host__ __device__ __forceinline__ int axis_nb(int c, int n, bool periodic) {
+    if (periodic) {
+        if (c < 0) return c + n;
+        if (c >= n) return c - n;
+        return c;
+    }
+    return (c < 0 || c >= n) ? -1 : c;
+}
+
+// Same for halo coordinates that may lie several lattice lengths away
+// (tile halos on small periodic axes): full modulo.
+__host__ __device__ __forceinline__ int axis_halo(int c, int n, bool periodic) {
+    if (periodic) {
+        int m = c % n;
+        return m < 0 ? m + n : m;
+    }
+    return (c < 0 || c >= n) ? -1 : c;
+}
+
+} // namespace ssmd

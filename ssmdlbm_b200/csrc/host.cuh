@@ -1,0 +1,198 @@
+// host.cuh — host-side helpers shared by the API and the per-lattice kernel TUs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/ssmd.h"
+#include "bulk.cuh"
+#include "init.cuh"
+#include "reduce.cuh"
+#include "surface.cuh"
+
+namespace ssmd {
+namespace host {
+
+int fail(int code, const char *fmt, ...);
+int cuda_check(cudaError_t e, const char *what);
+
+// Bulk-kernel timing events of the calling thread (ssmd_profile_*); returns the
+// event pair for the next launch, or nulls when profiling is off or full.
+void profile_next(cudaEvent_t *before, cudaEvent_t *after);
+
+constexpr size_t kStatusOff = 0;
+constexpr size_t kRedOutOff = 256;
+constexpr size_t kPartialOff = 512;
+constexpr int kMaxRedBlocks = 1024;
+constexpr size_t kWorkspaceBytes = kPartialOff + sizeof(double) * kRedVals * kMaxRedBlocks;
+
+inline size_t storage_size(int s) { return s == SSMD_STORAGE_F32 ? 4 : 2; }
+
+inline Geometry make_geometry(const ssmd_params &p) {
+    Geometry G{};
+    G.nx = p.nx;
+    G.ny = p.ny;
+    G.nz = p.nz;
+    G.nxy = p.nx * p.ny;
+    G.cells = (uint64_t)p.nx * p.ny * p.nz;
+    G.bcx = p.bc_x;
+    G.bcy = p.bc_y;
+    G.bcz = p.bc_z;
+    auto lohi = [](int bc, uint32_t n, int &lo, int &hi) {
+        lo = bc == SSMD_BC_PERIODIC ? 0 : 1;
+        hi = bc == SSMD_BC_PERIODIC ? (int)n - 1 : (int)n - 2;
+    };
+    lohi(p.bc_x, p.nx, G.x_lo, G.x_hi);
+    lohi(p.bc_y, p.ny, G.y_lo, G.y_hi);
+    lohi(p.bc_z, p.nz, G.z_lo, G.z_hi);
+    return G;
+}
+
+inline Physics make_physics(const ssmd_params &p) {
+    Physics P{};
+    P.nu_water = p.nu_water;
+    P.nu_oil_minus_water = p.nu_oil - p.nu_water; // FP32, as the reference's constexpr difference
+    P.omco_water = p.omco_water;
+    P.omco_oil = p.omco_oil;
+    P.omco_ref = p.omco_ref;
+    P.sigma = p.sigma;
+    P.gamma = p.gamma;
+    P.omega_g = p.omega_g;
+    P.u_oil = p.u_oil;
+    P.oil_cx = p.oil_cx;
+    P.oil_cy = p.oil_cy;
+    P.oil_r2 = p.oil_r2;
+    P.u_water = p.u_water;
+    P.water_cx = p.water_cx;
+    P.water_cz = p.water_cz;
+    P.water_r2 = p.water_r2;
+    P.noise_amp = p.noise_amp;
+    P.seed = p.seed;
+    return P;
+}
+
+inline Fields make_fields(const LBMFields &f) {
+    Fields F{};
+    F.rho = f.rho;
+    F.ux = f.ux;
+    F.uy = f.uy;
+    F.uz = f.uz;
+    F.pxx = f.pxx;
+    F.pyy = f.pyy;
+    F.pzz = f.pzz;
+    F.pxy = f.pxy;
+    F.pxz = f.pxz;
+    F.pyz = f.pyz;
+    F.phi = f.phi;
+    return F;
+}
+
+inline DeviceStatus *status_of(const ssmd_params &p) {
+    return reinterpret_cast<DeviceStatus *>(static_cast<char *>(p.workspace) + kStatusOff);
+}
+
+inline int check_fields(const ssmd_params &p, const LBMFields *f) {
+    if (!f) return fail(SSMD_ERR_INVALID_ARGUMENT, "fields is null");
+    const void *need[] = {f->rho, f->ux, f->uy, f->uz, f->pxx, f->pyy, f->pzz, f->pxy, f->pxz,
+                          f->pyz, f->phi, f->f, f->g, p.f_alt, p.g_alt, p.workspace};
+    const char *names[] = {"rho", "ux", "uy", "uz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz",
+                           "phi", "f", "g", "f_alt", "g_alt", "workspace"};
+    for (int i = 0; i < 16; ++i)
+        if (!need[i]) return fail(SSMD_ERR_INVALID_ARGUMENT, "device pointer %s is null", names[i]);
+    if (p.workspace_bytes < kWorkspaceBytes)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "workspace_bytes %zu < required %zu",
+                    p.workspace_bytes, kWorkspaceBytes);
+    return SSMD_OK;
+}
+
+static __global__ void set_status_kernel(DeviceStatus *s, unsigned long long step) {
+    s->flags = 0u;
+    s->step = step;
+    s->work_next = 0u;
+}
+
+// Bulk tiling: 32 x 8 columns, z chunks sized for >= ~8 resident waves of
+// work items on 148 SMs unless the caller fixes tile_z.
+inline void tiling(const ssmd_params &p, const Geometry &G, int &tiles_x, int &tiles_y, int &zchunk,
+            int &nchunks) {
+    tiles_x = (int)((G.nx + kTX - 1) / kTX);
+    tiles_y = (int)((G.ny + kTY - 1) / kTY);
+    const int nzf = G.z_hi - G.z_lo + 1;
+    if (p.tile_z > 0) {
+        zchunk = p.tile_z;
+    } else {
+        const int target = 148 * 2 * 4;
+        int want = (target + tiles_x * tiles_y - 1) / (tiles_x * tiles_y);
+        if (want < 1) want = 1;
+        zchunk = (nzf + want - 1) / want;
+        if (zchunk < 8) zchunk = 8;
+        if (zchunk > 64) zchunk = 64;
+    }
+    if (zchunk > nzf) zchunk = nzf;
+    nchunks = (nzf + zchunk - 1) / zchunk;
+}
+
+template <int Q, class T>
+int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32_t flags,
+                cudaStream_t st) {
+    StepArgs<T, T> a{};
+    a.geo = make_geometry(p);
+    a.phys = make_physics(p);
+    a.fld = make_fields(fl);
+    const bool even = (step & 1ull) == 0ull;
+    a.f_src = static_cast<const T *>(even ? fl.f : p.f_alt);
+    a.f_dst = static_cast<T *>(even ? p.f_alt : fl.f);
+    a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
+    a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
+    a.status = status_of(p);
+    a.flags = flags;
+    tiling(p, a.geo, a.tiles_x, a.tiles_y, a.zchunk, a.nzchunks);
+
+    const dim3 blk(kTX, kTY);
+    const unsigned nblk = (unsigned)(a.tiles_x * a.tiles_y * a.nzchunks);
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    profile_next(&ev0, &ev1);
+    if (ev0) cudaEventRecord(ev0, st);
+    bulk_kernel<Q, T, T><<<nblk, blk, 0, st>>>(a);
+    if (ev1) cudaEventRecord(ev1, st);
+    if (int e = cuda_check(cudaGetLastError(), "bulk_kernel launch")) return e;
+
+    const Geometry &G = a.geo;
+    const dim3 b2(32, 4);
+    auto grid2 = [&](uint32_t n0, uint32_t n1) {
+        return dim3((n0 + b2.x - 1) / b2.x, (n1 + b2.y - 1) / b2.y);
+    };
+    if (G.bcy == BC_JET) bc_water_inflow<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+    if (G.bcz == BC_JET) bc_oil_inflow<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+    if (G.bcy == BC_JET) bc_outflow_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+    if (G.bcz == BC_JET) bc_outflow_z<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+    if (G.bcx == BC_COPY) bc_copy_x<Q, T, T><<<grid2(G.ny, G.nz), b2, 0, st>>>(a);
+    if (G.bcy == BC_COPY) bc_copy_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+    return cuda_check(cudaGetLastError(), "boundary kernel launch");
+}
+
+template <int Q, class T>
+int launch_init_pops(const ssmd_params &p, const LBMFields &fl, cudaStream_t st) {
+    const Geometry G = make_geometry(p);
+    const unsigned nb = (unsigned)((G.cells + 255) / 256);
+    init_populations_kernel<Q, T, T><<<nb, 256, 0, st>>>(G, make_fields(fl), static_cast<T *>(fl.f),
+                                                          static_cast<T *>(p.f_alt),
+                                                          static_cast<T *>(fl.g),
+                                                          static_cast<T *>(p.g_alt));
+    return cuda_check(cudaGetLastError(), "init_populations launch");
+}
+
+
+#define SSMD_INSTANTIATE(Q, T)                                                                     \
+    template int launch_step<Q, T>(const ssmd_params &, const LBMFields &, uint64_t, uint32_t,      \
+                                   cudaStream_t);                                                   \
+    template int launch_init_pops<Q, T>(const ssmd_params &, const LBMFields &, cudaStream_t);
+
+#define SSMD_DECLARE(Q, T)                                                                         \
+    extern template int launch_step<Q, T>(const ssmd_params &, const LBMFields &, uint64_t,        \
+                                          uint32_t, cudaStream_t);                                  \
+    extern template int launch_init_pops<Q, T>(const ssmd_params &, const LBMFields &, cudaStream_t);
+
+} // namespace host
+} // namespace ssmd
