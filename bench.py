@@ -143,6 +143,9 @@ def workload(storage: int, q: int = Q):
                            w_in=0.05, noise=0.01, seed=1, storage=storage)
 
 
+STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
+
+
 def time_graph(sim, steps: int, warmup: int, world: int):
     """Device time of `steps` steps replayed as 2-step graphs (max over ranks)."""
     import torch
@@ -245,7 +248,7 @@ def run_ours(a, world, rank, local):
     from ssmdlbm_b200 import _lib
     from ssmdlbm_b200.lbm import Simulation
 
-    p = workload(_lib.STORAGE_F32)
+    p = workload(STORAGE_NAMES[a.storage], a.vs)
     sim = Simulation(p)
     sim.init()
     with ClockSampler(local) as clk:
@@ -257,7 +260,8 @@ def run_ours(a, world, rank, local):
 
     # live roofline of the dominant kernel
     bulk_ms = bulk_launch_ms(sim, 40)
-    bytes_per_launch = b_alg(Q, 4) * sim.cells
+    s_f0 = 4 if a.storage == "f32" else 2
+    bytes_per_launch = b_alg(a.vs, s_f0) * sim.cells
     peak, peak_kind = hbm_peak()
     achieved = bytes_per_launch / (bulk_ms * 1e-3) / 1e9
     n_bc = 2 + 0  # oil inflow + outflow z (x, y exact periodic: no ghost copies)
@@ -290,15 +294,15 @@ def run_ours(a, world, rank, local):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt * 1e3 / a.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: quiescent water + noisy oil inlet (the reference's initial state)",
-        "config": {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, FP32 storage, nozzle 16, tau 0.52, "
-                               "w 0.05 + 1% noise, seed 1",
-                   "cells": NX * NY * NZ, "velocity_set": "D3Q27", "storage": "f32",
+        "config": {"workload": f"oil jet D3Q{a.vs}+D3Q7 {NX}x{NY}x{NZ}, {a.storage} storage, nozzle 16, "
+                               "tau 0.52, w 0.05 + 1% noise, seed 1",
+                   "cells": NX * NY * NZ, "velocity_set": f"D3Q{a.vs}", "storage": a.storage,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (populations 0.9 GB per buffer)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
-                     "peak_kind": peak_kind, "kernel": "ssmd::bulk_kernel<27,float,float>",
-                     "bytes_per_cell": b_alg(Q, 4), "launch_ms": round(bulk_ms, 4)},
+                     "peak_kind": peak_kind, "kernel": f"ssmd::bulk_kernel<{a.vs},{a.storage}>",
+                     "bytes_per_cell": b_alg(a.vs, s_f0), "launch_ms": round(bulk_ms, 4)},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": a.steps * (1 + n_bc),
@@ -307,7 +311,7 @@ def run_ours(a, world, rank, local):
         "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
     }
     if rank == 0 and world == 1 and not a.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(workload(_lib.STORAGE_F32), steps=3)
+        line["cpu_baseline"] = cpu_baseline(workload(_lib.STORAGE_F32, a.vs), steps=3)
     return line
 
 
@@ -351,7 +355,13 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quick", action="store_true", help="skip the storage / velocity-set variants")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--size", default=None, help="nx,ny,nz of a smaller lattice (profiling runs)")
+    ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
+    ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
     a = ap.parse_args()
+    if a.size:
+        global NX, NY, NZ
+        NX, NY, NZ = (int(v) for v in a.size.split(","))
     if a.steps % 2:
         a.steps += 1
     a.warmup = max(a.warmup, 4)
