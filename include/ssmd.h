@@ -245,6 +245,22 @@ int ssmd_reduce(const ssmd_params *p, const LBMFields *fields, uint64_t steps_do
                 ssmd_stats *out, ssmd_stream_t stream);
 
 /*
+ * ssmd_reduce without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory (a plugin handed
+ * the fields by the host application with no memory of its own, or code that
+ * must not call cudaMalloc because it synchronises the device or a capture is
+ * open): p->workspace is not used; the partial sums live in a fixed 41 KiB
+ * array inside the library (512 partials of 10 doubles + result, per GPU,
+ * held until exit).  Every lattice ssmd_validate accepts fits; a larger
+ * partial count is refused.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array: overlapping calls race.  Same results as ssmd_reduce
+ * up to FP64 summation order; synchronises the stream.
+ */
+int ssmd_reduce_static(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done,
+                       ssmd_stats *out, ssmd_stream_t stream);
+
+/*
  * Copies the current populations (after `steps_done` steps) to the
  * reference's push layout: which = 0 -> hydrodynamic f (element type of the
  * storage), which = 1 -> g.  out has ssmd_f_bytes / ssmd_g_bytes bytes.

@@ -101,6 +101,8 @@ SIGNATURES = [
     ("ssmd_graph_launch", c_int32, [c_void_p, c_void_p]),
     ("ssmd_graph_destroy", c_int32, [c_void_p]),
     ("ssmd_reduce", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, POINTER(Stats), c_void_p]),
+    ("ssmd_reduce_static", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, POINTER(Stats),
+                                     c_void_p]),
     ("ssmd_populations_to_push", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_int32,
                                            c_void_p, c_void_p]),
     ("ssmd_check_status", c_int32, [POINTER(Params), POINTER(c_uint32), c_void_p]),

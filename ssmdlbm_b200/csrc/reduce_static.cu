@@ -1,0 +1,121 @@
+// reduce_static.cu — the global reductions without any device allocation.
+//
+// ssmd_reduce keeps its per-block partial sums in the caller's workspace
+// buffer.  Some callers cannot provide one: a monitoring or post-processing
+// plugin that is handed the simulation's LBMFields by the host application
+// but owns no device memory of its own, or code running where cudaMalloc is
+// off limits (it synchronises the whole device and is illegal while a stream
+// is being captured).  ssmd_reduce_static serves them: the same two reduction
+// kernels, with the partial sums and the result in a fixed array that lives
+// in this library's own device image.
+//
+// Limits and sharing rules:
+//   * the array holds kStaticPartials = 512 partial sums of kRedVals doubles
+//     plus one result row (41 KiB per GPU that loads the library, held until
+//     the process exits).  The first pass launches at most 512 blocks that
+//     stride over the cells, so every lattice the library accepts
+//     (nx*ny*nz <= 2^32 - 1, checked by ssmd_validate) fits; a partial count
+//     above 512 is refused with SSMD_ERR_INVALID_ARGUMENT.
+//   * every call on a device uses the same array and leaves its contents
+//     behind.  Pass 1 overwrites every partial that pass 2 reads and pass 2
+//     overwrites the result row, so nothing has to start at zero.  Calls that
+//     overlap on the GPU (different streams or threads at the same time) race
+//     on the array and corrupt each other's results: serialise them.
+//   * the device address of the array is looked up once per device with
+//     cudaGetSymbolAddress on the first call made while that device is
+//     current; make that first call before any stream capture.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "host.cuh"
+
+using namespace ssmd;
+using namespace ssmd::host;
+
+namespace {
+
+constexpr int kStaticPartials = 512;
+constexpr int kMaxDevices = 64;
+
+// [0, kRedVals * kStaticPartials): partials; last kRedVals doubles: result.
+static __device__ __align__(256) double g_reduce_scratch[kRedVals * (kStaticPartials + 1)];
+
+std::mutex g_setup_mutex;
+double *g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_reduce_scratch on the current device (set-up on first use).
+int scratch_address(double **out) {
+    int dev = 0;
+    if (int e = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return e;
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail(SSMD_ERR_UNSUPPORTED, "device index %d above %d", dev, kMaxDevices - 1);
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void *ptr = nullptr;
+        if (int e = cuda_check(cudaGetSymbolAddress(&ptr, g_reduce_scratch),
+                               "cudaGetSymbolAddress(reduction scratch)"))
+            return e;
+        g_scratch_ptr[dev] = static_cast<double *>(ptr);
+    }
+    *out = g_scratch_ptr[dev];
+    return SSMD_OK;
+}
+
+template <class T>
+int reduce_static(const ssmd_params &p, const LBMFields &fl, uint64_t steps_done, double *out_host,
+                  cudaStream_t st) {
+    const Geometry G = make_geometry(p);
+    const T *g = static_cast<const T *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
+    const uint64_t want = (G.cells + kRedThreads - 1) / kRedThreads;
+    const int nb = (int)(want < (uint64_t)kStaticPartials ? want : kStaticPartials);
+    if (nb > kStaticPartials)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "reduction needs %d partial sums, static scratch holds %d",
+                    nb, kStaticPartials);
+    double *scratch = nullptr;
+    if (int e = scratch_address(&scratch)) return e;
+    double *partials = scratch;
+    double *result = scratch + (size_t)kRedVals * kStaticPartials;
+    reduce_pass1<T><<<nb, kRedThreads, 0, st>>>(G, make_fields(fl), g, partials);
+    reduce_pass2<<<1, kRedThreads, 0, st>>>(partials, nb, result);
+    if (int e = cuda_check(cudaGetLastError(), "static reduce launch")) return e;
+    if (int e = cuda_check(cudaMemcpyAsync(out_host, result, sizeof(double) * kRedVals,
+                                           cudaMemcpyDeviceToHost, st),
+                           "static reduce copy"))
+        return e;
+    return cuda_check(cudaStreamSynchronize(st), "static reduce sync");
+}
+
+} // namespace
+
+extern "C" int ssmd_reduce_static(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done,
+                                  ssmd_stats *out, ssmd_stream_t stream) {
+    if (!out || !fields) return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    if (int e = ssmd_validate(p)) return e;
+    const void *need[] = {fields->rho, fields->ux, fields->uy, fields->uz, fields->phi, fields->g, p->g_alt};
+    for (const void *q : need)
+        if (!q) return fail(SSMD_ERR_INVALID_ARGUMENT, "a field, g or g_alt pointer is null");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    double v[kRedVals];
+    int e;
+    switch (p->storage) {
+    case SSMD_STORAGE_F32: e = reduce_static<float>(*p, *fields, steps_done, v, st); break;
+    case SSMD_STORAGE_F16: e = reduce_static<__half>(*p, *fields, steps_done, v, st); break;
+    default: e = reduce_static<__nv_bfloat16>(*p, *fields, steps_done, v, st); break;
+    }
+    if (e) return e;
+    out->phi_sum = v[0];
+    out->phi_sum_next = v[1];
+    out->mass = v[2];
+    out->momentum[0] = v[3];
+    out->momentum[1] = v[4];
+    out->momentum[2] = v[5];
+    out->kinetic = v[6];
+    out->u_max = v[7];
+    out->nonfinite = v[8];
+    out->cells = v[9];
+    if (v[8] > 0.0 || v[7] > (double)p->u_limit)
+        return fail(SSMD_ERR_UNSTABLE, "unstable state: %g non-finite cells, max |u| = %g (limit %g)",
+                    v[8], v[7], (double)p->u_limit);
+    return SSMD_OK;
+}
