@@ -12,7 +12,7 @@ import os
 from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_size_t, c_uint32, c_uint64, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libssmd.so")
+LIB_PATH = os.environ.get("SSMD_LIB") or os.path.join(HERE, "libssmd.so")
 
 SSMD_OK = 0
 SSMD_ERR_INVALID_ARGUMENT = 1

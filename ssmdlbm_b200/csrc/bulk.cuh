@@ -24,6 +24,10 @@
 
 namespace ssmd {
 
+#ifndef SSMD_BULK_MIN_BLOCKS
+#define SSMD_BULK_MIN_BLOCKS 3 // resident work items per SM the register budget targets
+#endif
+
 constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
 constexpr int kHX = kTX + 4, kHY = kTY + 4; // phi ring (halo 2)
 constexpr int kNX = kTX + 2, kNY = kTY + 2; // normal ring (halo 1)
@@ -34,28 +38,36 @@ struct BulkSmem {
     float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
 };
 
-__device__ __forceinline__ int ring5(int p) { return ((p % 5) + 5) % 5; }
-__device__ __forceinline__ int ring3(int p) { return ((p % 3) + 3) % 3; }
+// Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
+__device__ __forceinline__ int ring5(int p) { return (int)((unsigned)(p + 10) % 5u); }
+__device__ __forceinline__ int ring3(int p) { return (int)((unsigned)(p + 9) % 3u); }
 
 template <int Q, class TF, class TG>
 struct Bulk {
     using A = StepArgs<TF, TG>;
 
-    // phi^n at one cell, from the post-stream phase populations (pull layout).
-    static __device__ __forceinline__ float phi_from_g(const A &a, int x, int y, int z) {
+    // phi^n at fluid cell (x, y, z) with linear index c, from the post-stream
+    // phase populations (pull layout: direction q is read at c - c_q).
+    static __device__ __forceinline__ float phi_from_g(const A &a, int x, int y, int z, uint32_t c) {
         const Geometry &G = a.geo;
-        const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
-        const int xm = axis_nb(x - 1, G.nx, px), xp = axis_nb(x + 1, G.nx, px);
-        const int ym = axis_nb(y - 1, G.ny, py), yp = axis_nb(y + 1, G.ny, py);
-        const int zm = axis_nb(z - 1, G.nz, pz), zp = axis_nb(z + 1, G.nz, pz);
-        const uint32_t c = cell_index(G, x, y, z);
-        float s = Store<TG>::ld(a.g_src + slot(G, 0, c));
-        s += Store<TG>::ld(a.g_src + slot(G, 1, cell_index(G, xm, y, z)));
-        s += Store<TG>::ld(a.g_src + slot(G, 2, cell_index(G, xp, y, z)));
-        s += Store<TG>::ld(a.g_src + slot(G, 3, cell_index(G, x, ym, z)));
-        s += Store<TG>::ld(a.g_src + slot(G, 4, cell_index(G, x, yp, z)));
-        s += Store<TG>::ld(a.g_src + slot(G, 5, cell_index(G, x, y, zm)));
-        s += Store<TG>::ld(a.g_src + slot(G, 6, cell_index(G, x, y, zp)));
+        const int64_t N = (int64_t)G.cells, sy = G.nx, sz = G.nxy;
+        // Offsets of the source cells (pull: direction q is read at c - c_q); a
+        // fluid cell only wraps on an exact-periodic axis, handled by a per-lane
+        // correction instead of a branch so that a warp never runs two paths.
+        const int64_t wxm = (x == 0) ? (int64_t)G.nx : 0;                 // c - 1 wraps to +nx-1
+        const int64_t wxp = (x == (int)G.nx - 1) ? -(int64_t)G.nx : 0;
+        const int64_t wym = (y == 0) ? (int64_t)G.nxy : 0;
+        const int64_t wyp = (y == (int)G.ny - 1) ? -(int64_t)G.nxy : 0;
+        const int64_t wzm = (z == 0) ? N : 0;
+        const int64_t wzp = (z == (int)G.nz - 1) ? -N : 0;
+        const TG *pg = a.g_src + c;
+        float s = Store<TG>::ld(pg);
+        s += Store<TG>::ld(pg + (1 * N - 1 + wxm));
+        s += Store<TG>::ld(pg + (2 * N + 1 + wxp));
+        s += Store<TG>::ld(pg + (3 * N - sy + wym));
+        s += Store<TG>::ld(pg + (4 * N + sy + wyp));
+        s += Store<TG>::ld(pg + (5 * N - sz + wzm));
+        s += Store<TG>::ld(pg + (6 * N + sz + wzp));
         return s;
     }
 
@@ -64,22 +76,31 @@ struct Bulk {
                z <= G.z_hi;
     }
 
+    // Halo coordinate along one axis: one conditional wrap suffices unless the
+    // host flagged an axis shorter than the tile halo (halo_mod).
+    static __device__ __forceinline__ int halo_axis(const A &a, int c, int n, bool periodic) {
+        if (a.halo_mod) return axis_halo(c, n, periodic);
+        return axis_nb(c, n, periodic);
+    }
+
     // Fill ring slot of plane pz with phi over the tile + 2-cell halo.
     static __device__ void fill_phi(const A &a, BulkSmem &S, int x0, int y0, int pz, int tid) {
         const Geometry &G = a.geo;
-        const int gz = axis_halo(pz, G.nz, G.bcz == BC_PERIODIC);
+        const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
         const int s = ring5(pz);
+        const bool zfluid = gz >= G.z_lo && gz <= G.z_hi;
         for (int i = tid; i < kHX * kHY; i += kThreads) {
             const int hx = i % kHX, hy = i / kHX;
-            const int gx = axis_halo(x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
-            const int gy = axis_halo(y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
+            const int gx = halo_axis(a, x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
+            const int gy = halo_axis(a, y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
             float raw = 0.f, zer = 0.f;
             if (gx >= 0 && gy >= 0 && gz >= 0) {
-                if (fluid(G, gx, gy, gz)) {
-                    raw = phi_from_g(a, gx, gy, gz);
+                const uint32_t c = cell_index(G, gx, gy, gz);
+                if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
+                    raw = phi_from_g(a, gx, gy, gz, c);
                     zer = raw;
                 } else {
-                    raw = a.fld.phi[cell_index(G, gx, gy, gz)];
+                    raw = a.fld.phi[c];
                 }
             }
             S.phiR[s][hy][hx] = raw;
@@ -91,9 +112,8 @@ struct Bulk {
     // set's weights (phaseField.cuh:158-218); (hx, hy) is the centre in ring
     // coordinates, p0 the centre plane.
     template <class Ring>
-    static __device__ __forceinline__ void grad(const Ring &R, int hx, int hy, int p0, float &gx,
-                                                float &gy, float &gz) {
-        const int sm = ring5(p0 - 1), s0 = ring5(p0), sp = ring5(p0 + 1);
+    static __device__ __forceinline__ void grad(const Ring &R, int hx, int hy, int sm, int s0, int sp,
+                                                float &gx, float &gy, float &gz) {
         auto at = [&](int dx, int dy, int dz) -> float {
             const int sl = dz < 0 ? sm : (dz > 0 ? sp : s0);
             return R[sl][hy + dy][hx + dx];
@@ -119,7 +139,7 @@ struct Bulk {
         for (int i = tid; i < kNX * kNY; i += kThreads) {
             const int nxh = i % kNX, nyh = i / kNX;
             float gx, gy, gz;
-            grad(S.phiZ, nxh + 1, nyh + 1, pz, gx, gy, gz);
+            grad(S.phiZ, nxh + 1, nyh + 1, ring5(pz - 1), ring5(pz), ring5(pz + 1), gx, gy, gz);
             const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
             const float inv = 1.0f / (ind + 1e-9f);
             S.nrm[s][0][nyh][nxh] = gx * inv;
@@ -135,30 +155,7 @@ struct Bulk {
         const Geometry &G = a.geo;
         const Physics &P = a.phys;
         const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
-        // pull sources: direction with c = +1 reads the cell at -1
-        const uint32_t X[3] = {(uint32_t)axis_nb(x + 1, G.nx, px), (uint32_t)x,
-                               (uint32_t)axis_nb(x - 1, G.nx, px)};
-        const uint32_t Y[3] = {(uint32_t)axis_nb(y + 1, G.ny, py) * G.nx, (uint32_t)y * G.nx,
-                               (uint32_t)axis_nb(y - 1, G.ny, py) * G.nx};
-        const uint32_t Z[3] = {(uint32_t)axis_nb(z + 1, G.nz, pz) * G.nxy, (uint32_t)z * G.nxy,
-                               (uint32_t)axis_nb(z - 1, G.nz, pz) * G.nxy};
-        const uint32_t c0 = X[1] + Y[1] + Z[1];
-
-        // ---- gather f^n (issued first so the loads overlap the stencil work)
-        float f[Q];
-        unroll<0, Q>([&](auto q) {
-            constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
-            const uint32_t src = X[1 + cx] + Y[1 + cy] + Z[1 + cz];
-            f[q] = Store<TF>::ld(a.f_src + slot(G, q, src));
-        });
-        float gin[7];
-        if (a.phys.omega_g != 1.0f) {
-            unroll<0, 7>([&](auto q) {
-                constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
-                const uint32_t src = X[1 + cx] + Y[1 + cy] + Z[1 + cz];
-                gin[q] = Store<TG>::ld(a.g_src + slot(G, q, src));
-            });
-        }
+        const uint32_t c0 = cell_index(G, x, y, z);
 
         // ---- surface tension from the zeroed-ghost field (phaseField.cuh:246-293)
         const int hx = tx + 2, hy = ty + 2; // phi ring centre
@@ -185,13 +182,56 @@ struct Bulk {
         const float fy = stc * nat(1, 0, 0, 0);
         const float fz = stc * nat(2, 0, 0, 0);
 
-        // ---- normals of the phase update from phi with ghost values (lbm.cu:157-224)
-        float gx, gy, gz;
-        grad(S.phiR, hx, hy, z, gx, gy, gz);
-        const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
-        const float inv = 1.0f / (ind + 1e-9f);
-        const float nx = gx * inv, ny = gy * inv, nz = gz * inv;
+        // ---- normals of the phase update from phi with ghost values (lbm.cu:157-224).
+        // Away from ghost layers the raw and zeroed fields agree on the 3x3x3
+        // neighbourhood, so the ring's normal is the same number.
+        const bool near_ghost = (!px && (x <= G.x_lo || x >= G.x_hi)) ||
+                                (!py && (y <= G.y_lo || y >= G.y_hi)) ||
+                                (!pz && (z <= G.z_lo || z >= G.z_hi));
+        float nx = nat(0, 0, 0, 0), ny = nat(1, 0, 0, 0), nz = nat(2, 0, 0, 0);
+        if (near_ghost) {
+            float gx, gy, gz;
+            grad(S.phiR, hx, hy, ring5(z - 1), ring5(z), ring5(z + 1), gx, gy, gz);
+            const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
+            const float inv = 1.0f / (ind + 1e-9f);
+            nx = gx * inv;
+            ny = gy * inv;
+            nz = gz * inv;
+        }
         const float phi = S.phiR[ring5(z)][hy][hx];
+
+        // ---- gather f^n (after the stencil work, so that the Q values are live
+        // only across the moments and the collision).  The source of direction q
+        // is c0 - (cx + cy nx + cz nx ny), one warp-uniform offset per q, plus a
+        // per-lane correction where an exact-periodic axis wraps (no branch, so
+        // the warp holding the wrapping lane does not run two gathers).
+        const int64_t N = (int64_t)G.cells, sy = G.nx, sz = G.nxy;
+        const int64_t wxm = (px && x == 0) ? (int64_t)G.nx : 0; // source x-1 -> x-1+nx
+        const int64_t wxp = (px && x == (int)G.nx - 1) ? -(int64_t)G.nx : 0;
+        const int64_t wym = (py && y == 0) ? (int64_t)G.nxy : 0;
+        const int64_t wyp = (py && y == (int)G.ny - 1) ? -(int64_t)G.nxy : 0;
+        const int64_t wzm = (pz && z == 0) ? N : 0;
+        const int64_t wzp = (pz && z == (int)G.nz - 1) ? -N : 0;
+        auto src_off = [&](auto q) -> int64_t {
+            constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
+            int64_t o = (int64_t)q * N - (cx + cy * sy + cz * sz);
+            if constexpr (cx > 0) o += wxm;
+            if constexpr (cx < 0) o += wxp;
+            if constexpr (cy > 0) o += wym;
+            if constexpr (cy < 0) o += wyp;
+            if constexpr (cz > 0) o += wzm;
+            if constexpr (cz < 0) o += wzp;
+            return o;
+        };
+        float f[Q];
+        const TF *pf = a.f_src + c0;
+        unroll<0, Q>([&](auto q) { f[q] = Store<TF>::ld(pf + src_off(q)); });
+        float gin[7];
+        const bool bgk = a.phys.omega_g != 1.0f;
+        if (bgk) {
+            const TG *pg = a.g_src + c0;
+            unroll<0, 7>([&](auto q) { gin[q] = Store<TG>::ld(pg + src_off(q)); });
+        }
 
         // ---- hydrodynamics
         const Moments m = moments<Q>(f, fx, fy, fz);
@@ -199,7 +239,8 @@ struct Bulk {
         const float omega = 1.0f / (0.5f + 3.0f * nu);
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
-        unroll<0, Q>([&](auto q) { Store<TF>::st(a.f_dst + slot(G, q, c0), fo[q]); });
+        TF *pfd = a.f_dst + c0;
+        unroll<0, Q>([&](auto q) { Store<TF>::st(pfd + (int64_t)q * N, fo[q]); });
 
         // ---- conservative Allen-Cahn update, D3Q7 (lbm.cu:256-269; D3Q7.cuh:124-148)
         const float sharp = P.gamma * phi * (1.0f - phi);
@@ -214,12 +255,13 @@ struct Bulk {
         go[4] = kW7_1 * (phi - ay);
         go[5] = kW7_1 * (phi + az);
         go[6] = kW7_1 * (phi - az);
-        if (a.phys.omega_g != 1.0f) {
+        if (bgk) {
             // BGK with the anti-diffusion flux inside the equilibrium; omega_g = 1
             // reduces to the reference's g = g_eq + h.
             unroll<0, 7>([&](auto q) { go[q] = gin[q] + P.omega_g * (go[q] - gin[q]); });
         }
-        unroll<0, 7>([&](auto q) { Store<TG>::st(a.g_dst + slot(G, q, c0), go[q]); });
+        TG *pgd = a.g_dst + c0;
+        unroll<0, 7>([&](auto q) { Store<TG>::st(pgd + (int64_t)q * N, go[q]); });
 
         // ---- macroscopic fields needed by the boundaries (or all, on save steps)
         const bool bplane = (G.bcx == BC_COPY && (x == 1 || x == (int)G.nx - 2)) ||
@@ -243,7 +285,7 @@ struct Bulk {
 };
 
 template <int Q, class TF, class TG>
-__global__ void __launch_bounds__(kThreads, 2) bulk_kernel(const StepArgs<TF, TG> a) {
+__global__ void __launch_bounds__(kThreads, SSMD_BULK_MIN_BLOCKS) bulk_kernel(const StepArgs<TF, TG> a) {
     using B = Bulk<Q, TF, TG>;
     __shared__ BulkSmem S;
     const Geometry &G = a.geo;

@@ -85,6 +85,7 @@ struct StepArgs {
     uint32_t flags;       // SSMD_STEP_*
     int tiles_x, tiles_y; // bulk tiling
     int zchunk, nzchunks;
+    int halo_mod;         // 1: a tile halo may wrap a periodic axis more than once
 };
 
 // ------------------------------------------------------------- indexing

@@ -112,22 +112,49 @@ static __global__ void set_status_kernel(DeviceStatus *s, unsigned long long ste
     s->work_next = 0u;
 }
 
-// Bulk tiling: 32 x 8 columns, z chunks sized for >= ~8 resident waves of
-// work items on 148 SMs unless the caller fixes tile_z.
-inline void tiling(const ssmd_params &p, const Geometry &G, int &tiles_x, int &tiles_y, int &zchunk,
-            int &nchunks) {
+// Resident bulk work items per SM for this instantiation (queried once per
+// device and kernel) and the SM count.
+template <int Q, class T>
+inline void bulk_slots(int &per_sm, int &sms) {
+    static thread_local int cached_dev = -1, cached_per_sm = 0, cached_sms = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != cached_dev) {
+        int n = 0, m = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bulk_kernel<Q, T, T>, kThreads, 0) !=
+            cudaSuccess)
+            n = 1;
+        if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) m = 148;
+        cached_dev = dev;
+        cached_per_sm = n > 0 ? n : 1;
+        cached_sms = m > 0 ? m : 1;
+    }
+    per_sm = cached_per_sm;
+    sms = cached_sms;
+}
+
+// Bulk tiling: 32 x 8 columns; the z chunk minimises (waves of work items) x
+// (planes per item + the 3-plane ring prologue) unless the caller fixes tile_z.
+inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tiles_x, int &tiles_y,
+                   int &zchunk, int &nchunks) {
     tiles_x = (int)((G.nx + kTX - 1) / kTX);
     tiles_y = (int)((G.ny + kTY - 1) / kTY);
     const int nzf = G.z_hi - G.z_lo + 1;
+    const long cols = (long)tiles_x * tiles_y;
     if (p.tile_z > 0) {
         zchunk = p.tile_z;
     } else {
-        const int target = 148 * 2 * 4;
-        int want = (target + tiles_x * tiles_y - 1) / (tiles_x * tiles_y);
-        if (want < 1) want = 1;
-        zchunk = (nzf + want - 1) / want;
-        if (zchunk < 8) zchunk = 8;
-        if (zchunk > 64) zchunk = 64;
+        double best = 1e300;
+        zchunk = nzf;
+        for (int zc = 4; zc <= nzf; ++zc) {
+            const long nch = (nzf + zc - 1) / zc;
+            const long waves = (cols * nch + slots - 1) / slots;
+            const double t = (double)waves * (zc + 3);
+            if (t < best * (1.0 - 1e-9)) {
+                best = t;
+                zchunk = zc;
+            }
+        }
     }
     if (zchunk > nzf) zchunk = nzf;
     nchunks = (nzf + zchunk - 1) / zchunk;
@@ -147,7 +174,12 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
     a.status = status_of(p);
     a.flags = flags;
-    tiling(p, a.geo, a.tiles_x, a.tiles_y, a.zchunk, a.nzchunks);
+    int per_sm = 1, sms = 1;
+    bulk_slots<Q, T>(per_sm, sms);
+    tiling(p, a.geo, per_sm * sms, a.tiles_x, a.tiles_y, a.zchunk, a.nzchunks);
+    a.halo_mod = (a.geo.bcx == BC_PERIODIC && a.geo.nx < (uint32_t)(kTX + 4)) ||
+                 (a.geo.bcy == BC_PERIODIC && a.geo.ny < (uint32_t)(kTY + 4)) ||
+                 (a.geo.bcz == BC_PERIODIC && a.geo.nz < 6u);
 
     const dim3 blk(kTX, kTY);
     const unsigned nblk = (unsigned)(a.tiles_x * a.tiles_y * a.nzchunks);
