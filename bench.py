@@ -248,8 +248,11 @@ def run_ours(a, world, rank, local):
     from ssmdlbm_b200 import _lib
     from ssmdlbm_b200.lbm import Simulation
 
+    from ssmdlbm_b200 import autotune
     p = workload(STORAGE_NAMES[a.storage], a.vs)
+    p.bulk_path = a.path
     sim = Simulation(p)
+    tuned = autotune.tune(sim) if (a.path == 0 and not a.no_tune) else None
     sim.init()
     with ClockSampler(local) as clk:
         dt = time_graph(sim, a.steps, a.warmup, world)
@@ -265,6 +268,7 @@ def run_ours(a, world, rank, local):
     peak, peak_kind = hbm_peak()
     achieved = bytes_per_launch / (bulk_ms * 1e-3) / 1e9
     n_bc = 2 + 0  # oil inflow + outflow z (x, y exact periodic: no ghost copies)
+    sim_path, sim_tz = int(sim.p.bulk_path), int(sim.p.tile_z)
     sim.close()
     del sim
     torch.cuda.empty_cache()
@@ -275,17 +279,20 @@ def run_ours(a, world, rank, local):
                              ("d3q19_f32", 19, _lib.STORAGE_F32), ("d3q19_f16", 19, _lib.STORAGE_F16)):
             pv = workload(stg, q)
             sv = Simulation(pv)
+            tv = autotune.tune(sv) if (a.path == 0 and not a.no_tune) else None
             sv.init()
             dv = time_graph(sv, a.steps, a.warmup, world)
             bm = bulk_launch_ms(sv, 20)
             s_f = 4 if stg == _lib.STORAGE_F32 else 2
             variants[name] = {"mlups": round(sv.cells * a.steps / dv / 1e6, 1),
+                              "bulk_path": int(sv.p.bulk_path), "tile_z": int(sv.p.tile_z),
                               "bulk_ms": round(bm, 4),
                               "roofline_frac": round(b_alg(q, s_f) * sv.cells / (bm * 1e-3) / 1e9 / peak, 4)}
             sv.close()
             del sv
             torch.cuda.empty_cache()
 
+    p.bulk_path, p.tile_z = sim_path, sim_tz
     e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
     e2e_mlups = e2e_mlups * world
 
@@ -298,6 +305,8 @@ def run_ours(a, world, rank, local):
                                "tau 0.52, w 0.05 + 1% noise, seed 1",
                    "cells": NX * NY * NZ, "velocity_set": f"D3Q{a.vs}", "storage": a.storage,
                    "parallelism": f"replicas x{world}",
+                   "bulk_path": sim_path, "tile_z": sim_tz,
+                   "autotuned": tuned is not None,
                    "l2": "inputs larger than L2 (populations 0.9 GB per buffer)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
@@ -358,6 +367,9 @@ def main() -> int:
     ap.add_argument("--size", default=None, help="nx,ny,nz of a smaller lattice (profiling runs)")
     ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="bulk kernel path: 0 auto, 1 gathers, 2 TMA phi boxes, 3 TMA population slabs")
     a = ap.parse_args()
     if a.size:
         global NX, NY, NZ

@@ -65,6 +65,14 @@ typedef struct CUgraphExec_st *ssmd_graph_exec_t;
 #define SSMD_STORAGE_F16 1  /* f - w_q and g as IEEE half (round to nearest) */
 #define SSMD_STORAGE_BF16 2 /* f - w_q and g as bfloat16 (round to nearest)  */
 
+/* ------------------------------------------------- bulk kernel variants */
+#define SSMD_PATH_AUTO 0   /* library choice (currently SSMD_PATH_GATHER)        */
+#define SSMD_PATH_GATHER 1 /* per-cell loads of populations and of the phi halo */
+#define SSMD_PATH_TMA 2    /* TMA boxes of g for the phi halo                    */
+#define SSMD_PATH_SLAB 3   /* TMA slabs of the populations, one plane ahead      */
+/* (the TMA paths return SSMD_ERR_UNSUPPORTED unless nx * element size is a
+ * multiple of 16 bytes) */
+
 /* ------------------------------------------------------------ step flags */
 #define SSMD_STEP_STORE_MACROS 1u /* write rho, ux, uy, uz, phi at every cell */
 
@@ -142,7 +150,8 @@ typedef struct ssmd_params {
     size_t workspace_bytes;
 
     int32_t tile_z;   /* z planes per bulk work item (0: library default)     */
-    int32_t reserved[7];
+    int32_t bulk_path; /* SSMD_PATH_*: how the bulk kernel feeds the phi halo */
+    int32_t reserved[6];
 } ssmd_params;
 
 /* Global reductions, accumulated in FP64 over the fluid (non-ghost) cells. */

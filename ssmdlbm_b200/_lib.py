@@ -30,6 +30,11 @@ STORAGE_BF16 = 2
 
 STEP_STORE_MACROS = 1
 
+PATH_AUTO = 0
+PATH_GATHER = 1
+PATH_TMA = 2
+PATH_SLAB = 3
+
 
 class LBMFields(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in (
@@ -49,7 +54,7 @@ class Params(ctypes.Structure):
         ("u_water", c_float), ("water_cx", c_float), ("water_cz", c_float), ("water_r2", c_float),
         ("noise_amp", c_float), ("u_limit", c_float), ("seed", c_uint64),
         ("f_alt", c_void_p), ("g_alt", c_void_p), ("workspace", c_void_p), ("workspace_bytes", c_size_t),
-        ("tile_z", c_int32), ("reserved", c_int32 * 7),
+        ("tile_z", c_int32), ("bulk_path", c_int32), ("reserved", c_int32 * 6),
     ]
 
     def copy(self) -> "Params":

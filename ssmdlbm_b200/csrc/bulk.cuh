@@ -21,6 +21,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ssmd {
 
@@ -31,6 +32,36 @@ namespace ssmd {
 constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
 constexpr int kHX = kTX + 4, kHY = kTY + 4; // phi ring (halo 2)
 constexpr int kNX = kTX + 2, kNY = kTY + 2; // normal ring (halo 1)
+
+// Shared-memory boxes of g for the phi halo, filled by TMA: per stage, one box
+// per D3Q7 direction q, kHY rows x WX columns starting at
+// (x0 - XH, y0 - 2 - c_qy, plane - c_qz), so that the value direction q
+// contributes to halo cell (hx, hy) sits at row hy, column hx + XH - 2 - c_qx.
+template <class TG>
+struct GBox {
+    static constexpr int XH = 16 / (int)sizeof(TG); // halo columns: 16-byte aligned box start
+    static constexpr int WX = kTX + 2 * XH;
+    static constexpr int BOX = WX * kHY;                       // elements per box
+    static constexpr uint32_t BOX_BYTES = BOX * sizeof(TG);     // multiple of 128
+    static constexpr uint32_t STAGE_BYTES = 7 * BOX_BYTES;
+    static constexpr size_t SMEM = 2 * (size_t)STAGE_BYTES + 64; // two stages + barriers + flag
+};
+
+// Shared-memory slabs of the populations of one z plane, filled by TMA (the
+// slab path): per direction q one box of kTY rows x WX columns starting at
+// (x0 - XH or x0, y0 - c_qy, z - c_qz), so the value cell (tx, ty) pulls from
+// direction q sits at row ty, column tx - c_qx + (c_qx < 0 ? 0 : XH).
+template <class T>
+struct Slab {
+    static constexpr int XH = 16 / (int)sizeof(T); // 16-byte aligned left start
+    static constexpr int WX = kTX + XH;
+    static constexpr int ELEMS = WX * kTY;
+    static constexpr uint32_t BYTES = ELEMS * sizeof(T); // multiple of 128
+    template <int cx>
+    static constexpr int col0() { return cx < 0 ? 1 : XH - cx; } // column of tx = 0
+    template <int Q>
+    static constexpr size_t smem() { return 2 * (size_t)(Q + 7) * BYTES + 64; }
+};
 
 struct BulkSmem {
     float phiR[5][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
@@ -50,24 +81,25 @@ struct Bulk {
     // phase populations (pull layout: direction q is read at c - c_q).
     static __device__ __forceinline__ float phi_from_g(const A &a, int x, int y, int z, uint32_t c) {
         const Geometry &G = a.geo;
-        const int64_t N = (int64_t)G.cells, sy = G.nx, sz = G.nxy;
-        // Offsets of the source cells (pull: direction q is read at c - c_q); a
-        // fluid cell only wraps on an exact-periodic axis, handled by a per-lane
-        // correction instead of a branch so that a warp never runs two paths.
-        const int64_t wxm = (x == 0) ? (int64_t)G.nx : 0;                 // c - 1 wraps to +nx-1
-        const int64_t wxp = (x == (int)G.nx - 1) ? -(int64_t)G.nx : 0;
-        const int64_t wym = (y == 0) ? (int64_t)G.nxy : 0;
-        const int64_t wyp = (y == (int)G.ny - 1) ? -(int64_t)G.nxy : 0;
-        const int64_t wzm = (z == 0) ? N : 0;
-        const int64_t wzp = (z == (int)G.nz - 1) ? -N : 0;
-        const TG *pg = a.g_src + c;
-        float s = Store<TG>::ld(pg);
-        s += Store<TG>::ld(pg + (1 * N - 1 + wxm));
-        s += Store<TG>::ld(pg + (2 * N + 1 + wxp));
-        s += Store<TG>::ld(pg + (3 * N - sy + wym));
-        s += Store<TG>::ld(pg + (4 * N + sy + wyp));
-        s += Store<TG>::ld(pg + (5 * N - sz + wzm));
-        s += Store<TG>::ld(pg + (6 * N + sz + wzp));
+        // 32-bit source cell indices (pull: direction q is read at c - c_q); a
+        // fluid cell only wraps on an exact-periodic axis, selected per lane
+        // (no branch, so a warp never runs two paths).  Population q of cell i
+        // is then one wide multiply-add away from the warp-uniform base g + q N.
+        const uint32_t xm = c + (x == 0 ? G.nx - 1 : (uint32_t)-1);
+        const uint32_t xp = c + (x == (int)G.nx - 1 ? (uint32_t)(1 - (int)G.nx) : 1u);
+        const uint32_t ym = c + (y == 0 ? G.nxy - G.nx : (uint32_t)-(int)G.nx);
+        const uint32_t yp = c + (y == (int)G.ny - 1 ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx);
+        const uint32_t zm = c + (z == 0 ? (uint32_t)(G.cells - G.nxy) : (uint32_t)-(int)G.nxy);
+        const uint32_t zp = c + (z == (int)G.nz - 1 ? (uint32_t)-(int64_t)(G.cells - G.nxy) : G.nxy);
+        const TG *g = a.g_src;
+        const uint64_t N = G.cells;
+        float s = Store<TG>::ld(g + c);
+        s += Store<TG>::ld(g + 1 * N + xm);
+        s += Store<TG>::ld(g + 2 * N + xp);
+        s += Store<TG>::ld(g + 3 * N + ym);
+        s += Store<TG>::ld(g + 4 * N + yp);
+        s += Store<TG>::ld(g + 5 * N + zm);
+        s += Store<TG>::ld(g + 6 * N + zp);
         return s;
     }
 
@@ -106,6 +138,90 @@ struct Bulk {
             S.phiR[s][hy][hx] = raw;
             S.phiZ[s][hy][hx] = zer;
         }
+    }
+
+    static __device__ __forceinline__ float tofloat(float v) { return v; }
+    static __device__ __forceinline__ float tofloat(__half v) { return __half2float(v); }
+    static __device__ __forceinline__ float tofloat(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+    // Same as fill_phi, with the g values of fluid cells taken from the TMA
+    // boxes of this plane; cells whose 7-point stencil wraps an exact-periodic
+    // axis (outside the boxes) fall back to the gather.
+    static __device__ void fill_phi_box(const A &a, BulkSmem &S, const TG *B, int x0, int y0, int pz,
+                                        int tid) {
+        using GB = GBox<TG>;
+        const Geometry &G = a.geo;
+        const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC;
+        const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
+        const int s = ring5(pz);
+        const bool zfluid = gz >= G.z_lo && gz <= G.z_hi;
+        for (int i = tid; i < kHX * kHY; i += kThreads) {
+            const int hx = i % kHX, hy = i / kHX;
+            const int rx = x0 - 2 + hx, ry = y0 - 2 + hy;
+            const int gx = halo_axis(a, rx, G.nx, px);
+            const int gy = halo_axis(a, ry, G.ny, py);
+            float raw = 0.f, zer = 0.f;
+            if (gx >= 0 && gy >= 0 && gz >= 0) {
+                const uint32_t c = cell_index(G, gx, gy, gz);
+                if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
+                    const bool edge = (px && (rx < 1 || rx > (int)G.nx - 2)) || (py && (ry < 1 || ry > (int)G.ny - 2));
+                    if (edge) {
+                        raw = phi_from_g(a, gx, gy, gz, c);
+                    } else {
+                        const int col = hy * GB::WX + hx + GB::XH - 2;
+                        raw = tofloat(B[0 * GB::BOX + col]);
+                        raw += tofloat(B[1 * GB::BOX + col - 1]);
+                        raw += tofloat(B[2 * GB::BOX + col + 1]);
+                        raw += tofloat(B[3 * GB::BOX + col]);
+                        raw += tofloat(B[4 * GB::BOX + col]);
+                        raw += tofloat(B[5 * GB::BOX + col]);
+                        raw += tofloat(B[6 * GB::BOX + col]);
+                    }
+                    zer = raw;
+                } else {
+                    raw = a.fld.phi[c];
+                }
+            }
+            S.phiR[s][hy][hx] = raw;
+            S.phiZ[s][hy][hx] = zer;
+        }
+    }
+
+    // Thread 0: TMA loads of the 7 g boxes phi of plane pz needs.
+    static __device__ void issue_boxes(const A &a, const CUtensorMap *map, TG *B, uint64_t *bar, int x0,
+                                       int y0, int pz) {
+        using GB = GBox<TG>;
+        const Geometry &G = a.geo;
+        const bool pzp = G.bcz == BC_PERIODIC;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(bar, GB::STAGE_BYTES);
+        unroll<0, 7>([&](auto q) {
+            constexpr int cy = cy27(q), cz = cz27(q);
+            const int zq = pzp ? axis_halo(pz - cz, G.nz, true) : pz - cz;
+            tma_load_4d(B + q * GB::BOX, map, x0 - GB::XH, y0 - 2 - cy, zq, q, bar);
+        });
+    }
+
+    // Thread 0: TMA loads of the population slabs of plane z (f, and g when the
+    // phase field relaxes with omega_g != 1).
+    static __device__ void issue_slabs(const A &a, const CUtensorMap *fmap, const CUtensorMap *gmap, TF *Fs,
+                                       TG *Gs, uint64_t *bar, int x0, int y0, int z) {
+        const Geometry &G = a.geo;
+        const bool pzp = G.bcz == BC_PERIODIC;
+        const bool bgk = a.phys.omega_g != 1.0f;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(bar, (uint32_t)(Q + (bgk ? 7 : 0)) * Slab<TF>::BYTES);
+        unroll<0, Q>([&](auto q) {
+            constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
+            const int zq = pzp ? axis_halo(z - cz, G.nz, true) : z - cz;
+            tma_load_4d(Fs + q * Slab<TF>::ELEMS, fmap, cx < 0 ? x0 : x0 - Slab<TF>::XH, y0 - cy, zq, q, bar);
+        });
+        if (bgk)
+            unroll<0, 7>([&](auto q) {
+                constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
+                const int zq = pzp ? axis_halo(z - cz, G.nz, true) : z - cz;
+                tma_load_4d(Gs + q * Slab<TG>::ELEMS, gmap, cx < 0 ? x0 : x0 - Slab<TG>::XH, y0 - cy, zq, q, bar);
+            });
     }
 
     // Isotropic gradient 3 sum_q w_q c_q phi(x + c_q) with the hydrodynamic
@@ -150,8 +266,10 @@ struct Bulk {
     }
 
     // Update of one fluid cell (x, y, z); (tx, ty) its position in the tile.
+    // fs / gs: this plane's population slabs (slab path) or null (gather path).
     static __device__ __forceinline__ void cell(const A &a, const BulkSmem &S, int x, int y, int z,
-                                                int tx, int ty) {
+                                                int tx, int ty, const TF *fs = nullptr,
+                                                const TG *gs = nullptr) {
         const Geometry &G = a.geo;
         const Physics &P = a.phys;
         const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
@@ -205,32 +323,59 @@ struct Bulk {
         // is c0 - (cx + cy nx + cz nx ny), one warp-uniform offset per q, plus a
         // per-lane correction where an exact-periodic axis wraps (no branch, so
         // the warp holding the wrapping lane does not run two gathers).
-        const int64_t N = (int64_t)G.cells, sy = G.nx, sz = G.nxy;
-        const int64_t wxm = (px && x == 0) ? (int64_t)G.nx : 0; // source x-1 -> x-1+nx
-        const int64_t wxp = (px && x == (int)G.nx - 1) ? -(int64_t)G.nx : 0;
-        const int64_t wym = (py && y == 0) ? (int64_t)G.nxy : 0;
-        const int64_t wyp = (py && y == (int)G.ny - 1) ? -(int64_t)G.nxy : 0;
-        const int64_t wzm = (pz && z == 0) ? N : 0;
-        const int64_t wzp = (pz && z == (int)G.nz - 1) ? -N : 0;
-        auto src_off = [&](auto q) -> int64_t {
+        // Source cell of direction q: c0 + DX[cx] + DY[cy] + DZ[cz] in 32 bits,
+        // the per-lane deltas already wrapped on exact-periodic axes.
+        const uint64_t N = G.cells;
+        const uint32_t dxm = (px && x == 0) ? G.nx - 1 : (uint32_t)-1;            // c_x = +1 reads x - 1
+        const uint32_t dxp = (px && x == (int)G.nx - 1) ? (uint32_t)(1 - (int)G.nx) : 1u;
+        const uint32_t dym = (py && y == 0) ? G.nxy - G.nx : (uint32_t)-(int)G.nx;
+        const uint32_t dyp = (py && y == (int)G.ny - 1) ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx;
+        const uint32_t dzm = (pz && z == 0) ? (uint32_t)(N - G.nxy) : (uint32_t)-(int)G.nxy;
+        const uint32_t dzp = (pz && z == (int)G.nz - 1) ? (uint32_t)-(int64_t)(N - G.nxy) : G.nxy;
+        auto src = [&](auto q) -> uint32_t {
             constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
-            int64_t o = (int64_t)q * N - (cx + cy * sy + cz * sz);
-            if constexpr (cx > 0) o += wxm;
-            if constexpr (cx < 0) o += wxp;
-            if constexpr (cy > 0) o += wym;
-            if constexpr (cy < 0) o += wyp;
-            if constexpr (cz > 0) o += wzm;
-            if constexpr (cz < 0) o += wzp;
-            return o;
+            uint32_t i = c0;
+            if constexpr (cx > 0) i += dxm;
+            if constexpr (cx < 0) i += dxp;
+            if constexpr (cy > 0) i += dym;
+            if constexpr (cy < 0) i += dyp;
+            if constexpr (cz > 0) i += dzm;
+            if constexpr (cz < 0) i += dzp;
+            return i;
         };
         float f[Q];
-        const TF *pf = a.f_src + c0;
-        unroll<0, Q>([&](auto q) { f[q] = Store<TF>::ld(pf + src_off(q)); });
         float gin[7];
         const bool bgk = a.phys.omega_g != 1.0f;
-        if (bgk) {
-            const TG *pg = a.g_src + c0;
-            unroll<0, 7>([&](auto q) { gin[q] = Store<TG>::ld(pg + src_off(q)); });
+        if (fs == nullptr) {
+            unroll<0, Q>([&](auto q) { f[q] = Store<TF>::ld(a.f_src + (uint64_t)q * N + src(q)); });
+            if (bgk) unroll<0, 7>([&](auto q) { gin[q] = Store<TG>::ld(a.g_src + (uint64_t)q * N + src(q)); });
+        } else {
+            // slab path: immediate shared-memory offsets; lanes whose source wraps an
+            // exact-periodic x or y axis (outside the slab) reload those directions
+            unroll<0, Q>([&](auto q) {
+                constexpr int cx = cx27(q);
+                f[q] = tofloat(fs[q * Slab<TF>::ELEMS + ty * Slab<TF>::WX + tx + Slab<TF>::template col0<cx>()]);
+            });
+            if (bgk)
+                unroll<0, 7>([&](auto q) {
+                    constexpr int cx = cx27(q);
+                    gin[q] = tofloat(gs[q * Slab<TG>::ELEMS + ty * Slab<TG>::WX + tx + Slab<TG>::template col0<cx>()]);
+                });
+            const bool wx0 = px && x == 0, wx1 = px && x == (int)G.nx - 1;
+            const bool wy0 = py && y == 0, wy1 = py && y == (int)G.ny - 1;
+            if (wx0 || wx1 || wy0 || wy1) {
+                unroll<0, Q>([&](auto q) {
+                    constexpr int cx = cx27(q), cy = cy27(q);
+                    const bool w = (cx > 0 && wx0) || (cx < 0 && wx1) || (cy > 0 && wy0) || (cy < 0 && wy1);
+                    if (w) f[q] = Store<TF>::ld(a.f_src + (uint64_t)q * N + src(q));
+                });
+                if (bgk)
+                    unroll<0, 7>([&](auto q) {
+                        constexpr int cx = cx27(q), cy = cy27(q);
+                        const bool w = (cx > 0 && wx0) || (cx < 0 && wx1) || (cy > 0 && wy0) || (cy < 0 && wy1);
+                        if (w) gin[q] = Store<TG>::ld(a.g_src + (uint64_t)q * N + src(q));
+                    });
+            }
         }
 
         // ---- hydrodynamics
@@ -239,8 +384,7 @@ struct Bulk {
         const float omega = 1.0f / (0.5f + 3.0f * nu);
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
-        TF *pfd = a.f_dst + c0;
-        unroll<0, Q>([&](auto q) { Store<TF>::st(pfd + (int64_t)q * N, fo[q]); });
+        unroll<0, Q>([&](auto q) { Store<TF>::st(a.f_dst + (uint64_t)q * N + c0, fo[q]); });
 
         // ---- conservative Allen-Cahn update, D3Q7 (lbm.cu:256-269; D3Q7.cuh:124-148)
         const float sharp = P.gamma * phi * (1.0f - phi);
@@ -260,8 +404,7 @@ struct Bulk {
             // reduces to the reference's g = g_eq + h.
             unroll<0, 7>([&](auto q) { go[q] = gin[q] + P.omega_g * (go[q] - gin[q]); });
         }
-        TG *pgd = a.g_dst + c0;
-        unroll<0, 7>([&](auto q) { Store<TG>::st(pgd + (int64_t)q * N, go[q]); });
+        unroll<0, 7>([&](auto q) { Store<TG>::st(a.g_dst + (uint64_t)q * N + c0, go[q]); });
 
         // ---- macroscopic fields needed by the boundaries (or all, on save steps)
         const bool bplane = (G.bcx == BC_COPY && (x == 1 || x == (int)G.nx - 2)) ||
@@ -284,9 +427,19 @@ struct Bulk {
     }
 };
 
-template <int Q, class TF, class TG>
-__global__ void __launch_bounds__(kThreads, SSMD_BULK_MIN_BLOCKS) bulk_kernel(const StepArgs<TF, TG> a) {
+// Waits for TMA stages are bounded: after kTmaWaitNs without completion the
+// block records status bit 1, waits (bounded again) for its own copies in
+// flight and returns.
+constexpr uint64_t kTmaWaitNs = 2000000000ull;
+
+// PATH: 1 = per-cell gathers, 2 = TMA boxes for the phi halo, 3 = TMA slabs
+// for the populations (phi halo by gathers).
+template <int Q, class TF, class TG, int PATH>
+__global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS)
+    bulk_kernel(const StepArgs<TF, TG> a, const __grid_constant__ CUtensorMap gmap,
+                const __grid_constant__ CUtensorMap fmap) {
     using B = Bulk<Q, TF, TG>;
+    using GB = GBox<TG>;
     __shared__ BulkSmem S;
     const Geometry &G = a.geo;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTX * ty;
@@ -303,16 +456,144 @@ __global__ void __launch_bounds__(kThreads, SSMD_BULK_MIN_BLOCKS) bulk_kernel(co
     const int x = x0 + tx, y = y0 + ty;
     const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
 
-    for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
-    __syncthreads();
-    B::fill_nrm(S, zs - 1, tid);
-    B::fill_nrm(S, zs, tid);
-    for (int z = zs; z < ze; ++z) {
-        B::fill_nrm(S, z + 1, tid);
+    if constexpr (PATH == 3) {
+        extern __shared__ __align__(128) unsigned char dyn3[];
+        using SL = Slab<TF>;
+        constexpr size_t STAGE = (size_t)(Q + 7) * SL::BYTES;
+        auto fstage = [&](int k) { return reinterpret_cast<TF *>(dyn3 + (k & 1) * STAGE); };
+        auto gstage = [&](int k) { return reinterpret_cast<TG *>(dyn3 + (k & 1) * STAGE + (size_t)Q * SL::BYTES); };
+        uint64_t *bars = reinterpret_cast<uint64_t *>(dyn3 + 2 * STAGE);
+        volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2);
+        int issued = 0, consumed = 0; // thread 0 only
+        if (tid == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            *abort_flag = 0;
+            fence_barrier_init();
+        }
         __syncthreads();
-        if (active) B::cell(a, S, x, y, z, tx, ty);
-        if (z + 1 < ze) B::fill_phi(a, S, x0, y0, z + 3, tid);
+        auto issue = [&](int z) {
+            if (tid == 0 && z < ze) {
+                const int k = z - zs;
+                B::issue_slabs(a, &fmap, &gmap, fstage(k), gstage(k), &bars[k & 1], x0, y0, z);
+                ++issued;
+            }
+        };
+        issue(zs);
+        for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
+        B::fill_nrm(S, zs - 1, tid);
+        B::fill_nrm(S, zs, tid);
+        bool ok = true;
+        for (int z = zs; z < ze; ++z) {
+            const int k = z - zs;
+            issue(z + 1);
+            B::fill_nrm(S, z + 1, tid);
+            if (tid == 0) {
+                if (!mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs)) *abort_flag = 1;
+                else ++consumed;
+            }
+            __syncthreads();
+            if (*abort_flag) {
+                ok = false;
+                break;
+            }
+            mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs); // complete: visibility
+            if (active) B::cell(a, S, x, y, z, tx, ty, fstage(k), gstage(k));
+            if (z + 1 < ze) B::fill_phi(a, S, x0, y0, z + 3, tid);
+            __syncthreads();
+        }
+        if (!ok && tid == 0) {
+            atomicOr(&a.status->flags, 2u);
+            for (int k = consumed; k < issued; ++k)
+                mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs);
+        }
+    } else if constexpr (PATH == 1) {
+        for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
+        __syncthreads();
+        B::fill_nrm(S, zs - 1, tid);
+        B::fill_nrm(S, zs, tid);
+        for (int z = zs; z < ze; ++z) {
+            B::fill_nrm(S, z + 1, tid);
+            __syncthreads();
+            if (active) B::cell(a, S, x, y, z, tx, ty);
+            if (z + 1 < ze) B::fill_phi(a, S, x0, y0, z + 3, tid);
+            __syncthreads();
+        }
+    } else {
+        extern __shared__ __align__(128) unsigned char dyn[];
+        TG *const stage0 = reinterpret_cast<TG *>(dyn);
+        TG *const stage1 = reinterpret_cast<TG *>(dyn + GB::STAGE_BYTES);
+        uint64_t *bars = reinterpret_cast<uint64_t *>(dyn + 2 * (size_t)GB::STAGE_BYTES);
+        volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2);
+        const int p_first = zs - 2;
+        const int p_last = max(zs + 2, ze + 1);
+        int issued = 0, consumed = 0; // thread 0 only
+        if (tid == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            *abort_flag = 0;
+            fence_barrier_init();
+        }
+        __syncthreads();
+        auto issue = [&](int p) {
+            if (tid == 0 && p <= p_last) {
+                const int k = p - p_first;
+                B::issue_boxes(a, &gmap, (k & 1) ? stage1 : stage0, &bars[k & 1], x0, y0, p);
+                ++issued;
+            }
+        };
+        // thread 0 polls (bounded), then everybody learns the outcome after a barrier
+        auto poll = [&](int p) {
+            if (tid == 0) {
+                const int k = p - p_first;
+                if (!mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs)) *abort_flag = 1;
+                else ++consumed;
+            }
+        };
+        auto confirm = [&](int p) {
+            const int k = p - p_first;
+            mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs); // already complete
+            return (k & 1) ? stage1 : stage0;
+        };
+        bool ok = true;
+        issue(p_first);
+        issue(p_first + 1);
+        for (int p = zs - 2; p <= zs + 2 && ok; ++p) {
+            poll(p);
+            __syncthreads();
+            if (*abort_flag) {
+                ok = false;
+                break;
+            }
+            B::fill_phi_box(a, S, confirm(p), x0, y0, p, tid);
+            __syncthreads();
+            issue(p + 2);
+        }
+        if (ok) {
+            B::fill_nrm(S, zs - 1, tid);
+            B::fill_nrm(S, zs, tid);
+            for (int z = zs; z < ze; ++z) {
+                B::fill_nrm(S, z + 1, tid);
+                const bool more = z + 1 < ze;
+                if (more) poll(z + 3);
+                __syncthreads();
+                if (*abort_flag) {
+                    ok = false;
+                    break;
+                }
+                if (active) B::cell(a, S, x, y, z, tx, ty);
+                if (more) B::fill_phi_box(a, S, confirm(z + 3), x0, y0, z + 3, tid);
+                __syncthreads();
+                if (more) issue(z + 5);
+            }
+        }
+        if (!ok && tid == 0) {
+            atomicOr(&a.status->flags, 2u);
+            // wait (bounded) for this block's copies still in flight before leaving
+            for (int k = consumed; k < issued; ++k)
+                mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs);
+        }
     }
 }
 

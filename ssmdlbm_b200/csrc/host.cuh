@@ -7,6 +7,7 @@
 
 #include "../../include/ssmd.h"
 #include "bulk.cuh"
+#include "tma.cuh"
 #include "init.cuh"
 #include "reduce.cuh"
 #include "surface.cuh"
@@ -112,16 +113,26 @@ static __global__ void set_status_kernel(DeviceStatus *s, unsigned long long ste
     s->work_next = 0u;
 }
 
+// Dynamic shared memory of a bulk instantiation (TMA boxes or slabs).
+template <int Q, class T, int PATH>
+constexpr size_t bulk_dyn_smem() {
+    return PATH == 2 ? GBox<T>::SMEM : (PATH == 3 ? Slab<T>::template smem<Q>() : 0);
+}
+
 // Resident bulk work items per SM for this instantiation (queried once per
-// device and kernel) and the SM count.
-template <int Q, class T>
+// device and kernel, after raising its dynamic shared-memory limit) and the
+// SM count.
+template <int Q, class T, int PATH>
 inline void bulk_slots(int &per_sm, int &sms) {
     static thread_local int cached_dev = -1, cached_per_sm = 0, cached_sms = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != cached_dev) {
         int n = 0, m = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bulk_kernel<Q, T, T>, kThreads, 0) !=
+        const size_t dyn = bulk_dyn_smem<Q, T, PATH>();
+        if (dyn > 0)
+            cudaFuncSetAttribute(bulk_kernel<Q, T, T, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bulk_kernel<Q, T, T, PATH>, kThreads, dyn) !=
             cudaSuccess)
             n = 1;
         if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) m = 148;
@@ -174,8 +185,21 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
     a.status = status_of(p);
     a.flags = flags;
+    // Kernel path: per-cell gathers (default), TMA boxes for the phi halo, or
+    // TMA slabs for the populations; the TMA paths need a 16-byte aligned x pitch.
+    CUtensorMap gmap{}, fmap{};
+    int path = p.bulk_path == SSMD_PATH_AUTO ? SSMD_PATH_GATHER : p.bulk_path;
+    if (path == SSMD_PATH_TMA &&
+        !encode_populations<T>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, GBox<T>::WX, kHY))
+        return fail(SSMD_ERR_UNSUPPORTED, "TMA path needs nx * element size to be a multiple of 16 bytes");
+    if (path == SSMD_PATH_SLAB &&
+        !(encode_populations<T>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, Slab<T>::WX, kTY) &&
+          encode_populations<T>(&fmap, a.f_src, a.geo.nx, a.geo.ny, a.geo.nz, Q, Slab<T>::WX, kTY)))
+        return fail(SSMD_ERR_UNSUPPORTED, "slab path needs nx * element size to be a multiple of 16 bytes");
     int per_sm = 1, sms = 1;
-    bulk_slots<Q, T>(per_sm, sms);
+    if (path == SSMD_PATH_TMA) bulk_slots<Q, T, 2>(per_sm, sms);
+    else if (path == SSMD_PATH_SLAB) bulk_slots<Q, T, 3>(per_sm, sms);
+    else bulk_slots<Q, T, 1>(per_sm, sms);
     tiling(p, a.geo, per_sm * sms, a.tiles_x, a.tiles_y, a.zchunk, a.nzchunks);
     a.halo_mod = (a.geo.bcx == BC_PERIODIC && a.geo.nx < (uint32_t)(kTX + 4)) ||
                  (a.geo.bcy == BC_PERIODIC && a.geo.ny < (uint32_t)(kTY + 4)) ||
@@ -186,7 +210,12 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     profile_next(&ev0, &ev1);
     if (ev0) cudaEventRecord(ev0, st);
-    bulk_kernel<Q, T, T><<<nblk, blk, 0, st>>>(a);
+    if (path == SSMD_PATH_TMA)
+        bulk_kernel<Q, T, T, 2><<<nblk, blk, bulk_dyn_smem<Q, T, 2>(), st>>>(a, gmap, fmap);
+    else if (path == SSMD_PATH_SLAB)
+        bulk_kernel<Q, T, T, 3><<<nblk, blk, bulk_dyn_smem<Q, T, 3>(), st>>>(a, gmap, fmap);
+    else
+        bulk_kernel<Q, T, T, 1><<<nblk, blk, 0, st>>>(a, gmap, fmap);
     if (ev1) cudaEventRecord(ev1, st);
     if (int e = cuda_check(cudaGetLastError(), "bulk_kernel launch")) return e;
 

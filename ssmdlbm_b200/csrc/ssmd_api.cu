@@ -161,6 +161,8 @@ int ssmd_validate(const ssmd_params *p) {
     for (float v : fl)
         if (!std::isfinite(v)) return fail(SSMD_ERR_INVALID_ARGUMENT, "non-finite parameter");
     if (p->tile_z < 0) return fail(SSMD_ERR_INVALID_ARGUMENT, "tile_z must be >= 0");
+    if (p->bulk_path < SSMD_PATH_AUTO || p->bulk_path > SSMD_PATH_SLAB)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "unknown bulk_path %d", p->bulk_path);
     return SSMD_OK;
 }
 

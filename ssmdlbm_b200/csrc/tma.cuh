@@ -1,0 +1,133 @@
+// tma.cuh — Tensor Memory Accelerator loads and mbarriers (sm_100a), no multicast.
+//
+// Device side: thin inline-PTX wrappers for mbarrier init / expect-tx /
+// try-wait and the 4-D tiled bulk tensor load into this CTA's shared memory.
+// Host side: encoding of a [q][z][y][x] population array as a 4-D tensor map
+// (x innermost) through the driver entry point cuTensorMapEncodeTiled.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+
+namespace ssmd {
+
+// ------------------------------------------------------------------ device
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Make barrier initialisation visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Order this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy writes into the same buffer.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: true when the phase completed, false after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
+// 4-D tiled load of one box (coordinates in elements, x innermost; x * size
+// must be a multiple of 16 bytes) into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int x, int y, int z, int q,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------------------ host
+template <class T>
+struct TmaType;
+template <>
+struct TmaType<float> {
+    static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+};
+template <>
+struct TmaType<__half> {
+    static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+};
+template <>
+struct TmaType<__nv_bfloat16> {
+    static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+};
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// [nq][nz][ny][nx] array of T as a 4-D tensor, boxes of box_x x box_y x 1 x 1.
+// Returns false when the layout cannot be described (row pitch not a multiple
+// of 16 bytes, misaligned base) or the encoder is unavailable.
+template <class T>
+inline bool encode_populations(CUtensorMap *map, const void *base, uint32_t nx, uint32_t ny, uint32_t nz,
+                               uint32_t nq, uint32_t box_x, uint32_t box_y) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const uint64_t es = sizeof(T);
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (nx * es) % 16 != 0 || (box_x * es) % 16 != 0)
+        return false;
+    const cuuint64_t dims[4] = {nx, ny, nz, nq};
+    const cuuint64_t strides[3] = {nx * es, (uint64_t)nx * ny * es, (uint64_t)nx * ny * nz * es};
+    const cuuint32_t box[4] = {box_x, box_y, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(map, TmaType<T>::value, 4, const_cast<void *>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+} // namespace ssmd

@@ -236,3 +236,36 @@ def test_reduced_storage_error_vs_fp64_oracle(storage, tol):
     errs = field_errors(sim_fields(sim), oracle_fields(o))
     print(storage, errs)
     assert max(errs.values()) <= tol, errs
+
+
+@pytest.mark.parametrize("vs,storage", [(19, _lib.STORAGE_F32), (27, _lib.STORAGE_F16)])
+def test_kernel_paths_agree_bitwise(vs, storage):
+    """The TMA-fed phi halo and the per-cell gather produce identical bits, on a
+    jet box whose tiles touch the periodic wrap and the inflow / outflow planes."""
+    p = configs.oil_jet(64, 40, 48, vs, tau=0.56, sigma=5e-3, mobility=0.1, diam=8, noise=0.01, seed=3,
+                        storage=storage)
+    out = []
+    for path in (_lib.PATH_GATHER, _lib.PATH_TMA, _lib.PATH_SLAB):
+        q = p.copy()
+        q.bulk_path = path
+        sim = _sim(q)
+        sim.init_from_macros(*seeded_macros((48, 40, 64), seed=6))
+        sim.step(6, store_macros=True)
+        assert sim.check_status() == 0
+        out.append((sim_fields(sim), sim.populations_push(0), sim.populations_push(1)))
+    for o in out[1:]:
+        for k in FIELDS:
+            assert np.array_equal(out[0][0][k], o[0][k]), k
+        assert np.array_equal(out[0][1], o[1]) and np.array_equal(out[0][2], o[2])
+
+
+def test_autotuner_picks_a_measured_candidate(tmp_path, monkeypatch):
+    from ssmdlbm_b200 import autotune
+    monkeypatch.setenv("SSMD_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    p = configs.oil_jet(64, 40, 48, 19, tau=0.56, sigma=5e-3, mobility=0.1, diam=8)
+    sim = _sim(p)
+    best = autotune.tune(sim, steps=2)
+    assert best["ms_per_step"] > 0 and len(best["tried"]) >= 3
+    assert (sim.p.bulk_path, sim.p.tile_z) == (best["bulk_path"], best["tile_z"])
+    again = autotune.tune(_sim(p))  # served from the cache
+    assert again["bulk_path"] == best["bulk_path"] and again["tile_z"] == best["tile_z"]
