@@ -290,6 +290,24 @@ int ssmd_profile_enable(int32_t max_launches);
 int ssmd_profile_read(float *ms, int32_t max, int32_t *count);
 int ssmd_profile_disable(void);
 
+/* ------------------------------------------------------------ output files
+ * The reference's file formats (host code, no GPU needed):
+ *   ssmd_output_bin:  <dir>/<name><step:06>.bin, count raw FP32 values
+ *                     (src/postProcess/PostProcess.cuh:44-98)
+ *   ssmd_output_vti:  <dir>/step_<step:06>.vti, VTK ImageData whose appended
+ *                     raw arrays are the existing <name><step>.bin files, in
+ *                     the given order (PostProcess.cuh:100-262)
+ *   ssmd_output_info: <dir>/<id>_info.txt run metadata
+ *                     (src/functions/hostFunctions.cuh:47-87)              */
+int ssmd_output_bin(const char *dir, const char *name, uint64_t step, const float *values,
+                    uint64_t count);
+int ssmd_output_vti(const char *dir, uint64_t step, uint32_t nx, uint32_t ny, uint32_t nz,
+                    const char *const *names, int32_t count);
+int ssmd_output_info(const char *dir, const char *id, const char *velocity_set, float u_water,
+                     float u_oil, double reynolds_water, double reynolds_oil, double weber,
+                     uint32_t nx, uint32_t ny, uint32_t nz, int32_t diam_water, int32_t diam_oil,
+                     int64_t nsteps, int64_t macro_save);
+
 /* Reads and clears the device status word (synchronises the stream):
  * bit 0 = a bulk cell produced a non-finite density. */
 int ssmd_check_status(const ssmd_params *p, uint32_t *status_out, ssmd_stream_t stream);

@@ -109,11 +109,38 @@ def build_ref_case(case: str, force: bool = False) -> str:
     return exe
 
 
+def vti_binary(case: str) -> str:
+    return os.path.join(REF_DIR, case, "vti_ref")
+
+
+def build_vti_case(case: str, force: bool = False) -> str:
+    """The reference's host-side .vti writer for the lattice of `case`."""
+    out_dir = os.path.join(REF_DIR, case)
+    build_ref_case(case, force)  # writes the case's constants.cuh
+    exe = vti_binary(case)
+    src = os.path.join(HERE, "ref_harness", "vti_ref.cu")
+    deps = [src, os.path.join(out_dir, "constants.cuh")]
+    if not force and os.path.exists(exe) and all(os.path.getmtime(d) <= os.path.getmtime(exe) for d in deps):
+        return exe
+    c = CASES[case]
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cmd = [nvcc, "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "--extended-lambda", "-std=c++20",
+           "-I", out_dir, "-I", REF_SRC, src, f"-DVS_{c['vs']}", f"-DENABLE_FP16={c['fp16']}",
+           "-DBENCHMARK=0", "-DTIME_AVERAGE=0", "-DREYNOLDS_MOMENTS=0", "-DVORTICITY_FIELDS=0",
+           "-DPASSIVE_SCALAR=0", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference vti writer build failed for {case}:\n{r.stdout}\n{r.stderr}")
+    return exe
+
+
 def build_ref(force: bool = False) -> list[str]:
     if not os.path.isdir(REF_SRC):
         return []
     with cf.ThreadPoolExecutor(max_workers=min(8, len(CASES))) as ex:
-        return list(ex.map(lambda k: build_ref_case(k, force), CASES))
+        out = list(ex.map(lambda k: build_ref_case(k, force), CASES))
+    out.append(build_vti_case("q19_s", force))
+    return out
 
 
 if __name__ == "__main__":

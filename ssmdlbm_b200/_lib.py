@@ -111,6 +111,11 @@ SIGNATURES = [
     ("ssmd_populations_to_push", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_int32,
                                            c_void_p, c_void_p]),
     ("ssmd_check_status", c_int32, [POINTER(Params), POINTER(c_uint32), c_void_p]),
+    ("ssmd_output_bin", c_int32, [c_char_p, c_char_p, c_uint64, c_void_p, c_uint64]),
+    ("ssmd_output_vti", c_int32, [c_char_p, c_uint64, c_uint32, c_uint32, c_uint32, POINTER(c_char_p), c_int32]),
+    ("ssmd_output_info", c_int32, [c_char_p, c_char_p, c_char_p, c_float, c_float, c_double, c_double,
+                                   c_double, c_uint32, c_uint32, c_uint32, c_int32, c_int32,
+                                   ctypes.c_int64, ctypes.c_int64]),
     ("ssmd_profile_enable", c_int32, [c_int32]),
     ("ssmd_profile_read", c_int32, [POINTER(c_float), c_int32, POINTER(c_int32)]),
     ("ssmd_profile_disable", c_int32, []),

@@ -25,7 +25,7 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xptxas", "-v"]
-SOURCES = ["ssmd_api.cu", "kernels_q19.cu", "kernels_q27.cu", "reduce_static.cu"]
+SOURCES = ["ssmd_api.cu", "kernels_q19.cu", "kernels_q27.cu", "reduce_static.cu", "output.cpp"]
 
 
 def nvcc() -> str:
@@ -38,7 +38,7 @@ def nvcc() -> str:
 def _deps() -> list[str]:
     out = [os.path.join(ROOT, "include", "ssmd.h")]
     for f in os.listdir(CSRC):
-        if f.endswith((".cu", ".cuh", ".h")):
+        if f.endswith((".cu", ".cuh", ".h", ".cpp")):
             out.append(os.path.join(CSRC, f))
     return out
 
