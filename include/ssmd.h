@@ -166,6 +166,16 @@ typedef struct ssmd_stats {
     double cells;        /* number of fluid cells reduced                     */
 } ssmd_stats;
 
+/* One connected component of phi > threshold (ssmd_droplets). */
+typedef struct ssmd_droplet {
+    uint32_t root;          /* smallest cell index of the component              */
+    uint32_t cells;         /* number of cells                                   */
+    double volume;          /* FP64 sum of phi over those cells                  */
+    uint32_t touches_inlet; /* 1 when it reaches the first fluid plane (z = 1 for
+                               inflow faces): the intact jet, not a droplet      */
+    uint32_t reserved;
+} ssmd_droplet;
+
 /* -------------------------------------------------------------- queries */
 int ssmd_abi_version(void);
 const char *ssmd_last_error(void);
@@ -289,6 +299,34 @@ int ssmd_populations_to_push(const ssmd_params *p, const LBMFields *fields,
 int ssmd_profile_enable(int32_t max_launches);
 int ssmd_profile_read(float *ms, int32_t max, int32_t *count);
 int ssmd_profile_disable(void);
+
+/* ------------------------------------------------------------ checkpoints
+ * Bit-exact save / resume (the reference's phi / rho dumps cannot restart a
+ * run): current populations, the eleven macroscopic arrays and the device
+ * step counter.  Loading requires the same lattice, velocity set, storage and
+ * face kinds, writes the populations into both buffers and returns the step
+ * count to continue from in *steps_done.  Both synchronise the stream.     */
+int ssmd_checkpoint_save(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done,
+                         const char *path, ssmd_stream_t stream);
+int ssmd_checkpoint_load(const ssmd_params *p, LBMFields *fields, const char *path,
+                         uint64_t *steps_done, ssmd_stream_t stream);
+
+/* ------------------------------------------------------------- statistics
+ * Both read the macroscopic arrays (a step with SSMD_STEP_STORE_MACROS first).
+ * ssmd_centreline: for every z, mean u_z and phi over the cells nearest the
+ *   oil-nozzle axis (oil_cx, oil_cy); uz_out and phi_out are DEVICE arrays of
+ *   nz doubles.  Asynchronous.
+ * ssmd_droplets: connected components (6-neighbour, exact-periodic axes wrap)
+ *   of fluid cells with phi > threshold; writes up to max_droplets entries to
+ *   the HOST array out (unordered) and the number found to *n_out
+ *   (SSMD_ERR_INVALID_ARGUMENT when more than max_droplets exist).  Needs
+ *   ssmd_droplets_scratch_bytes() bytes of device scratch.  Synchronises.  */
+int ssmd_centreline(const ssmd_params *p, const LBMFields *fields, double *uz_out, double *phi_out,
+                    ssmd_stream_t stream);
+size_t ssmd_droplets_scratch_bytes(const ssmd_params *p, int32_t max_droplets);
+int ssmd_droplets(const ssmd_params *p, const LBMFields *fields, float threshold, void *scratch,
+                  size_t scratch_bytes, ssmd_droplet *out, int32_t max_droplets, int32_t *n_out,
+                  ssmd_stream_t stream);
 
 /* ------------------------------------------------------------ output files
  * The reference's file formats (host code, no GPU needed):

@@ -36,6 +36,9 @@ def lib():
         L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.oracle_set.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.oracle_centreline.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_droplets.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.oracle_noise.restype = ctypes.c_double
         L.oracle_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
         _lib = L
@@ -88,6 +91,26 @@ class Oracle:
         v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
         if lib().oracle_set(self.h, FIELD_IDS[name], v.ctypes.data) != 0:
             raise KeyError(name)
+
+    def centreline(self):
+        uz = np.zeros(self.shape[0])
+        phi = np.zeros(self.shape[0])
+        lib().oracle_centreline(self.h, uz.ctypes.data, phi.ctypes.data)
+        return uz, phi
+
+    def droplets(self, threshold: float = 0.5, max_droplets: int = 100000):
+        """Components as a structured array (root, cells, volume, touches_inlet), sorted by root."""
+        root = np.zeros(max_droplets, np.uint32)
+        cells = np.zeros(max_droplets, np.uint32)
+        vol = np.zeros(max_droplets, np.float64)
+        touch = np.zeros(max_droplets, np.uint32)
+        n = ctypes.c_int()
+        lib().oracle_droplets(self.h, threshold, root.ctypes.data, cells.ctypes.data, vol.ctypes.data,
+                              touch.ctypes.data, max_droplets, ctypes.byref(n))
+        k = min(n.value, max_droplets)
+        out = np.zeros(k, dtype=[("root", "u4"), ("cells", "u4"), ("volume", "f8"), ("touches_inlet", "u4")])
+        out["root"], out["cells"], out["volume"], out["touches_inlet"] = root[:k], cells[:k], vol[:k], touch[:k]
+        return out
 
 
 def noise(seed: int, step: int, cell: int, stream: int = 0) -> float:

@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include <algorithm>
 
 #include "../include/ssmd.h"
 #include "../ssmdlbm_b200/csrc/noise.h"
@@ -645,6 +646,90 @@ int oracle_get(void *hv, int id, double *out) {
 int oracle_set(void *hv, int id, const float *in) {
     auto *h = static_cast<Handle *>(hv);
     return h->precision == 32 ? set_field(O<float>(h), id, in) : set_field(O<double>(h), id, in);
+}
+
+// Centreline mean of u_z and phi over the cells nearest the oil-nozzle axis
+// (the definition of ssmd_centreline), FP64, nz values each.
+int oracle_centreline(void *hv, double *uz_out, double *phi_out) {
+    auto *h = static_cast<Handle *>(hv);
+    auto run = [&](auto &o) {
+        const int x0 = (int)std::floor(o.p.oil_cx), x1 = (int)std::ceil(o.p.oil_cx);
+        const int y0 = (int)std::floor(o.p.oil_cy), y1 = (int)std::ceil(o.p.oil_cy);
+        for (int z = 0; z < o.nz; ++z) {
+            double su = 0, sp = 0;
+            int n = 0;
+            for (int y = y0; y <= y1; ++y)
+                for (int x = x0; x <= x1; ++x) {
+                    if (x < 0 || y < 0 || x >= o.nx || y >= o.ny) continue;
+                    su += (double)(float)o.uz[o.idx(x, y, z)];
+                    sp += (double)(float)o.phi[o.idx(x, y, z)];
+                    ++n;
+                }
+            uz_out[z] = n ? su / n : 0.0;
+            phi_out[z] = n ? sp / n : 0.0;
+        }
+    };
+    if (h->precision == 32) run(O<float>(h));
+    else run(O<double>(h));
+    return 0;
+}
+
+// Connected components of fluid cells with phi > thr (6-neighbour, exact
+// periodic axes wrap), by breadth-first search in index order, so the first
+// cell reached is the component's smallest index.  Per component: root, cell
+// count, FP64 sum of phi (as float, the precision the device reads) and
+// whether it reaches the first fluid plane.  Sorted by root.
+int oracle_droplets(void *hv, float thr, uint32_t *root, uint32_t *cells, double *vol, uint32_t *touch, int max,
+                    int *n_out) {
+    auto *h = static_cast<Handle *>(hv);
+    auto run = [&](auto &o) {
+        const int64_t N = o.N;
+        std::vector<float> phi(N);
+        for (int64_t i = 0; i < N; ++i) phi[i] = (float)o.phi[i];
+        auto fg = [&](int x, int y, int z) { return o.fluid(x, y, z) && phi[o.idx(x, y, z)] > thr; };
+        std::vector<uint8_t> seen(N, 0);
+        std::vector<int64_t> queue;
+        int n = 0;
+        for (int z = 0; z < o.nz; ++z)
+            for (int y = 0; y < o.ny; ++y)
+                for (int x = 0; x < o.nx; ++x) {
+                    const int64_t i = o.idx(x, y, z);
+                    if (seen[i] || !fg(x, y, z)) continue;
+                    uint32_t cnt = 0;
+                    double v = 0;
+                    uint32_t t = 0;
+                    queue.assign(1, i);
+                    seen[i] = 1;
+                    for (size_t k = 0; k < queue.size(); ++k) {
+                        const int64_t c = queue[k];
+                        const int cx = (int)(c % o.nx), cy = (int)((c / o.nx) % o.ny), cz = (int)(c / ((int64_t)o.nx * o.ny));
+                        ++cnt;
+                        v += (double)phi[c];
+                        if (cz == o.lo[2]) t = 1;
+                        const int d[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                        for (auto &e : d) {
+                            const int qx = o.nb(0, cx + e[0]), qy = o.nb(1, cy + e[1]), qz = o.nb(2, cz + e[2]);
+                            if (qx < 0 || qy < 0 || qz < 0 || !fg(qx, qy, qz)) continue;
+                            const int64_t j = o.idx(qx, qy, qz);
+                            if (!seen[j]) {
+                                seen[j] = 1;
+                                queue.push_back(j);
+                            }
+                        }
+                    }
+                    if (n < max) {
+                        root[n] = (uint32_t)i;
+                        cells[n] = cnt;
+                        vol[n] = v;
+                        touch[n] = t;
+                    }
+                    ++n;
+                }
+        *n_out = n;
+    };
+    if (h->precision == 32) run(O<float>(h));
+    else run(O<double>(h));
+    return 0;
 }
 
 double oracle_noise(uint64_t seed, uint64_t step, uint32_t cell, uint32_t stream) {

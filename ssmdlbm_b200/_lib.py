@@ -78,6 +78,11 @@ class Stats(ctypes.Structure):
         }
 
 
+class Droplet(ctypes.Structure):
+    _fields_ = [("root", c_uint32), ("cells", c_uint32), ("volume", c_double), ("touches_inlet", c_uint32),
+                ("reserved", c_uint32)]
+
+
 class SSMDError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"ssmd error {code}: {msg}")
@@ -111,6 +116,13 @@ SIGNATURES = [
     ("ssmd_populations_to_push", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_int32,
                                            c_void_p, c_void_p]),
     ("ssmd_check_status", c_int32, [POINTER(Params), POINTER(c_uint32), c_void_p]),
+    ("ssmd_checkpoint_save", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_char_p, c_void_p]),
+    ("ssmd_checkpoint_load", c_int32, [POINTER(Params), POINTER(LBMFields), c_char_p, POINTER(c_uint64),
+                                       c_void_p]),
+    ("ssmd_centreline", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_void_p, c_void_p]),
+    ("ssmd_droplets_scratch_bytes", c_size_t, [POINTER(Params), c_int32]),
+    ("ssmd_droplets", c_int32, [POINTER(Params), POINTER(LBMFields), c_float, c_void_p, c_size_t,
+                                POINTER(Droplet), c_int32, POINTER(c_int32), c_void_p]),
     ("ssmd_output_bin", c_int32, [c_char_p, c_char_p, c_uint64, c_void_p, c_uint64]),
     ("ssmd_output_vti", c_int32, [c_char_p, c_uint64, c_uint32, c_uint32, c_uint32, POINTER(c_char_p), c_int32]),
     ("ssmd_output_info", c_int32, [c_char_p, c_char_p, c_char_p, c_float, c_float, c_double, c_double,

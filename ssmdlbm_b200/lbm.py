@@ -126,6 +126,48 @@ class Simulation:
         d["status"] = code
         return d
 
+    def save(self, path: str) -> None:
+        """Bit-exact checkpoint of the lattice (populations, macroscopic arrays, step)."""
+        check(lib().ssmd_checkpoint_save(ctypes.byref(self.p), ctypes.byref(self.fields), self.steps_done,
+                                         str(path).encode(), self.stream))
+
+    def load(self, path: str) -> None:
+        """Resume from a checkpoint written by save() for the same lattice."""
+        n = ctypes.c_uint64()
+        torch.cuda.synchronize(self.device)
+        check(lib().ssmd_checkpoint_load(ctypes.byref(self.p), ctypes.byref(self.fields), str(path).encode(),
+                                         ctypes.byref(n), self.stream))
+        self.steps_done = int(n.value)
+
+    def centreline(self):
+        """Mean u_z and phi along the oil-nozzle axis, per z (FP64 numpy arrays).
+        Needs the macroscopic fields of a step with store_macros."""
+        uz = torch.zeros(int(self.p.nz), dtype=torch.float64, device=self.device)
+        phi = torch.zeros_like(uz)
+        torch.cuda.synchronize(self.device)
+        check(lib().ssmd_centreline(ctypes.byref(self.p), ctypes.byref(self.fields), uz.data_ptr(),
+                                    phi.data_ptr(), self.stream))
+        self.sync()
+        return uz.cpu().numpy(), phi.cpu().numpy()
+
+    def droplets(self, threshold: float = 0.5, max_droplets: int = 100000) -> np.ndarray:
+        """Connected components of phi > threshold (structured array sorted by
+        root: root, cells, volume, touches_inlet).  Needs store_macros fields."""
+        L = lib()
+        nbytes = int(L.ssmd_droplets_scratch_bytes(ctypes.byref(self.p), max_droplets))
+        scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        out = (_lib.Droplet * max_droplets)()
+        n = ctypes.c_int32()
+        torch.cuda.synchronize(self.device)
+        check(L.ssmd_droplets(ctypes.byref(self.p), ctypes.byref(self.fields), threshold, scratch.data_ptr(),
+                              nbytes, out, max_droplets, ctypes.byref(n), self.stream))
+        k = min(n.value, max_droplets)
+        arr = np.zeros(k, dtype=[("root", "u4"), ("cells", "u4"), ("volume", "f8"), ("touches_inlet", "u4")])
+        for i in range(k):
+            arr[i] = (out[i].root, out[i].cells, out[i].volume, out[i].touches_inlet)
+        arr.sort(order="root")
+        return arr
+
     def check_status(self) -> int:
         v = ctypes.c_uint32()
         check(lib().ssmd_check_status(ctypes.byref(self.p), ctypes.byref(v), self.stream))
