@@ -243,6 +243,34 @@ def cpu_baseline(p, steps: int = 3):
                       f"warm-up step ({dt:.1f} s)"}
 
 
+def run_sweep(steps: int = 40):
+    """The 48-lattice sweep (N x N x 4N, N in {32, 48, 64, 96}, seed 2; D3Q19
+    f32): batched persistent launches replayed as graphs, z-chunk height
+    tuned over {8, 16, 32}, against the same steps issued lattice by lattice."""
+    import torch
+    from ssmdlbm_b200.batch import Sweep, sweep_params
+    sw = Sweep(sweep_params(48, seed=2))
+    sw.init()
+    best = None
+    for tz in (8, 16, 32):
+        sw.set_tile_z(tz)
+        sw.timed(4)
+        dt = sw.timed(steps)
+        if best is None or dt < best[1]:
+            best = (tz, dt)
+    sw.set_tile_z(best[0])
+    sw.timed_one_by_one(4)
+    dt_single = sw.timed_one_by_one(steps)
+    out = {"lattices": sw.count, "cells": sw.cells, "steps": steps, "tile_z": best[0],
+           "batched_mlups": round(sw.cells * steps / best[1] / 1e6, 1),
+           "one_by_one_mlups": round(sw.cells * steps / dt_single / 1e6, 1),
+           "launches_per_step": {"batched": 3, "one_by_one": sw.count * 3}}
+    sw.close()
+    del sw
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(a, world, rank, local):
     import torch
     from ssmdlbm_b200 import _lib
@@ -292,6 +320,8 @@ def run_ours(a, world, rank, local):
             del sv
             torch.cuda.empty_cache()
 
+    sweep = run_sweep() if not a.quick else None
+
     p.bulk_path, p.tile_z = sim_path, sim_tz
     e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
     e2e_mlups = e2e_mlups * world
@@ -317,6 +347,7 @@ def run_ours(a, world, rank, local):
         "gpu_launches": a.steps * (1 + n_bc),
         "clocks": clocks,
         "variants": variants,
+        "sweep": sweep,
         "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
     }
     if rank == 0 and world == 1 and not a.no_cpu:

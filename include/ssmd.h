@@ -300,6 +300,25 @@ int ssmd_profile_enable(int32_t max_launches);
 int ssmd_profile_read(float *ms, int32_t max, int32_t *count);
 int ssmd_profile_disable(void);
 
+/* ------------------------------------------------------------ batched sweep
+ * Many independent lattices (a parameter sweep: different sizes, inlet
+ * speeds, nozzles, sigma, tau, mobility) advanced by ONE persistent bulk
+ * launch per step whose blocks pull (lattice, tile, z-chunk) work items from
+ * an atomic counter, plus one launch per boundary kind for all lattices.
+ * params[i] / fields[i] are complete single-lattice descriptions (own
+ * buffers and workspace); all share velocity set and storage.  The device
+ * table (ssmd_batch_table_bytes) is filled once by ssmd_batch_prepare
+ * (synchronous); the batch's z-chunk comes from params[i].tile_z (0: 16).
+ * ssmd_batch_step advances every lattice by one step (parity = step & 1, as
+ * ssmd_step); ssmd_batch_capture_graph captures an even number of them.   */
+size_t ssmd_batch_table_bytes(const ssmd_params *params, int32_t count);
+int ssmd_batch_prepare(const ssmd_params *params, const LBMFields *fields, int32_t count, void *table,
+                       size_t table_bytes, ssmd_stream_t stream);
+int ssmd_batch_step(const ssmd_params *params, int32_t count, uint64_t step, uint32_t flags, void *table,
+                    ssmd_stream_t stream);
+int ssmd_batch_capture_graph(const ssmd_params *params, int32_t count, uint64_t first_step, int32_t steps,
+                             uint32_t flags, void *table, ssmd_stream_t stream, ssmd_graph_exec_t *out);
+
 /* ------------------------------------------------------------ checkpoints
  * Bit-exact save / resume (the reference's phi / rho dumps cannot restart a
  * run): current populations, the eleven macroscopic arrays and the device

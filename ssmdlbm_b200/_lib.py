@@ -116,6 +116,11 @@ SIGNATURES = [
     ("ssmd_populations_to_push", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_int32,
                                            c_void_p, c_void_p]),
     ("ssmd_check_status", c_int32, [POINTER(Params), POINTER(c_uint32), c_void_p]),
+    ("ssmd_batch_table_bytes", c_size_t, [POINTER(Params), c_int32]),
+    ("ssmd_batch_prepare", c_int32, [POINTER(Params), POINTER(LBMFields), c_int32, c_void_p, c_size_t, c_void_p]),
+    ("ssmd_batch_step", c_int32, [POINTER(Params), c_int32, c_uint64, c_uint32, c_void_p, c_void_p]),
+    ("ssmd_batch_capture_graph", c_int32, [POINTER(Params), c_int32, c_uint64, c_int32, c_uint32, c_void_p,
+                                           c_void_p, POINTER(c_void_p)]),
     ("ssmd_checkpoint_save", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, c_char_p, c_void_p]),
     ("ssmd_checkpoint_load", c_int32, [POINTER(Params), POINTER(LBMFields), c_char_p, POINTER(c_uint64),
                                        c_void_p]),

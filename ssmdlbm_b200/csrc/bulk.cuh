@@ -202,6 +202,26 @@ struct Bulk {
         });
     }
 
+    // One work item on the gather path: the 32 x 8 column at (x0, y0) over
+    // planes [zs, ze).  Ends with a block-wide barrier.
+    static __device__ void run_gather(const A &a, BulkSmem &S, int x0, int y0, int zs, int ze, int tx, int ty,
+                                      int tid) {
+        const Geometry &G = a.geo;
+        const int x = x0 + tx, y = y0 + ty;
+        const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
+        for (int p = zs - 2; p <= zs + 2; ++p) fill_phi(a, S, x0, y0, p, tid);
+        __syncthreads();
+        fill_nrm(S, zs - 1, tid);
+        fill_nrm(S, zs, tid);
+        for (int z = zs; z < ze; ++z) {
+            fill_nrm(S, z + 1, tid);
+            __syncthreads();
+            if (active) cell(a, S, x, y, z, tx, ty);
+            if (z + 1 < ze) fill_phi(a, S, x0, y0, z + 3, tid);
+            __syncthreads();
+        }
+    }
+
     // Thread 0: TMA loads of the population slabs of plane z (f, and g when the
     // phase field relaxes with omega_g != 1).
     static __device__ void issue_slabs(const A &a, const CUtensorMap *fmap, const CUtensorMap *gmap, TF *Fs,
@@ -509,17 +529,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
                 mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs);
         }
     } else if constexpr (PATH == 1) {
-        for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
-        __syncthreads();
-        B::fill_nrm(S, zs - 1, tid);
-        B::fill_nrm(S, zs, tid);
-        for (int z = zs; z < ze; ++z) {
-            B::fill_nrm(S, z + 1, tid);
-            __syncthreads();
-            if (active) B::cell(a, S, x, y, z, tx, ty);
-            if (z + 1 < ze) B::fill_phi(a, S, x0, y0, z + 3, tid);
-            __syncthreads();
-        }
+        B::run_gather(a, S, x0, y0, zs, ze, tx, ty, tid);
     } else {
         extern __shared__ __align__(128) unsigned char dyn[];
         TG *const stage0 = reinterpret_cast<TG *>(dyn);

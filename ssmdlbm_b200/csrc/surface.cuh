@@ -74,11 +74,9 @@ __device__ __forceinline__ void regularized_slot(const StepArgs<TF, TG> &a, uint
 
 // Water inflow disc on y = 0 (BoundaryConditions.cuh:36-99).  Thread (x, z).
 template <int Q, class TF, class TG>
-__global__ void bc_water_inflow(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_water_inflow_at(const StepArgs<TF, TG> &a, const int x, const int z) {
     const Geometry &G = a.geo;
     const Physics &P = a.phys;
-    const int x = threadIdx.x + blockIdx.x * blockDim.x;
-    const int z = threadIdx.y + blockIdx.y * blockDim.y;
     if (x >= (int)G.nx || z >= (int)G.nz) return;
     const float dx = float(x) - P.water_cx, dz = float(z) - P.water_cz;
     if (dx * dx + dz * dz > P.water_r2) return;
@@ -103,11 +101,9 @@ __global__ void bc_water_inflow(const StepArgs<TF, TG> a) {
 
 // Oil inflow disc on z = 0 (BoundaryConditions.cuh:101-168).  Thread (x, y).
 template <int Q, class TF, class TG>
-__global__ void bc_oil_inflow(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_oil_inflow_at(const StepArgs<TF, TG> &a, const int x, const int y) {
     const Geometry &G = a.geo;
     const Physics &P = a.phys;
-    const int x = threadIdx.x + blockIdx.x * blockDim.x;
-    const int y = threadIdx.y + blockIdx.y * blockDim.y;
     if (x >= (int)G.nx || y >= (int)G.ny) return;
     const float dx = float(x) - P.oil_cx, dy = float(y) - P.oil_cy;
     if (dx * dx + dy * dy > P.oil_r2) return;
@@ -136,10 +132,8 @@ __global__ void bc_oil_inflow(const StepArgs<TF, TG> a) {
 
 // Outflow on y = ny-1 (BoundaryConditions.cuh:170-233).  Thread (x, z).
 template <int Q, class TF, class TG>
-__global__ void bc_outflow_y(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_outflow_y_at(const StepArgs<TF, TG> &a, const int x, const int z) {
     const Geometry &G = a.geo;
-    const int x = threadIdx.x + blockIdx.x * blockDim.x;
-    const int z = threadIdx.y + blockIdx.y * blockDim.y;
     if (!in_range(x, G.x_lo, G.x_hi) || !in_range(z, G.z_lo, G.z_hi)) return;
     const uint32_t b = cell_index(G, x, G.ny - 1, z);
     const uint32_t i1 = cell_index(G, x, G.ny - 2, z);
@@ -165,10 +159,8 @@ __global__ void bc_outflow_y(const StepArgs<TF, TG> a) {
 
 // Outflow on z = nz-1 (BoundaryConditions.cuh:235-293).  Thread (x, y).
 template <int Q, class TF, class TG>
-__global__ void bc_outflow_z(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_outflow_z_at(const StepArgs<TF, TG> &a, const int x, const int y) {
     const Geometry &G = a.geo;
-    const int x = threadIdx.x + blockIdx.x * blockDim.x;
-    const int y = threadIdx.y + blockIdx.y * blockDim.y;
     if (!in_range(x, G.x_lo, G.x_hi) || !in_range(y, G.y_lo, G.y_hi)) return;
     const uint32_t b = cell_index(G, x, y, G.nz - 1);
     const uint32_t i1 = cell_index(G, x, y, G.nz - 2);
@@ -198,10 +190,8 @@ __global__ void bc_outflow_z(const StepArgs<TF, TG> a) {
 // (nx-1, .) <- (2, .).  Slots whose pull home leaves the lattice are never
 // read by a fluid cell and are skipped.
 template <int Q, class TF, class TG>
-__global__ void bc_copy_x(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_copy_x_at(const StepArgs<TF, TG> &a, const int y, const int z) {
     const Geometry &G = a.geo;
-    const int y = threadIdx.x + blockIdx.x * blockDim.x;
-    const int z = threadIdx.y + blockIdx.y * blockDim.y;
     if (y >= (int)G.ny || z >= (int)G.nz) return;
     const int nx = G.nx;
     const bool py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
@@ -236,10 +226,8 @@ __global__ void bc_copy_x(const StepArgs<TF, TG> a) {
 // reference only has the x version; this completes the x,y-periodic jet box).
 // Thread (x, z), all x, z.
 template <int Q, class TF, class TG>
-__global__ void bc_copy_y(const StepArgs<TF, TG> a) {
+__device__ __forceinline__ void bc_copy_y_at(const StepArgs<TF, TG> &a, const int x, const int z) {
     const Geometry &G = a.geo;
-    const int x = threadIdx.x + blockIdx.x * blockDim.x;
-    const int z = threadIdx.y + blockIdx.y * blockDim.y;
     if (x >= (int)G.nx || z >= (int)G.nz) return;
     const int ny = G.ny;
     const bool px = G.bcx == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
@@ -268,6 +256,33 @@ __global__ void bc_copy_y(const StepArgs<TF, TG> a) {
     F.uy[gR] = F.uy[bL];
     F.uz[gL] = F.uz[bR];
     F.uz[gR] = F.uz[bL];
+}
+
+
+// ---- kernels: one thread per face cell (i0, i1) ------------------------------
+template <int Q, class TF, class TG>
+__global__ void bc_water_inflow(const StepArgs<TF, TG> a) {
+    bc_water_inflow_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
+}
+template <int Q, class TF, class TG>
+__global__ void bc_oil_inflow(const StepArgs<TF, TG> a) {
+    bc_oil_inflow_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
+}
+template <int Q, class TF, class TG>
+__global__ void bc_outflow_y(const StepArgs<TF, TG> a) {
+    bc_outflow_y_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
+}
+template <int Q, class TF, class TG>
+__global__ void bc_outflow_z(const StepArgs<TF, TG> a) {
+    bc_outflow_z_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
+}
+template <int Q, class TF, class TG>
+__global__ void bc_copy_x(const StepArgs<TF, TG> a) {
+    bc_copy_x_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
+}
+template <int Q, class TF, class TG>
+__global__ void bc_copy_y(const StepArgs<TF, TG> a) {
+    bc_copy_y_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
 }
 
 } // namespace ssmd
