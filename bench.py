@@ -145,6 +145,11 @@ def workload(storage: int, q: int = Q):
 
 STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
 
+# DRAM bytes per cell of one bulk launch, dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture (profiles/, 128 x 128 x 256 case,
+# scaled to the lattice by its cell count)
+NCU_BYTES_PER_CELL = {(27, "f32"): 277.3}
+
 
 def time_graph(sim, steps: int, warmup: int, world: int):
     """Device time of `steps` steps replayed as 2-step graphs (max over ranks)."""
@@ -339,7 +344,9 @@ def run_ours(a, world, rank, local):
                    "autotuned": tuned is not None,
                    "l2": "inputs larger than L2 (populations 0.9 GB per buffer)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": (int(NCU_BYTES_PER_CELL[(a.vs, a.storage)] * NX * NY * NZ)
+                                 if (a.vs, a.storage) in NCU_BYTES_PER_CELL else None),
                      "peak_kind": peak_kind, "kernel": f"ssmd::bulk_kernel<{a.vs},{a.storage}>",
                      "bytes_per_cell": b_alg(a.vs, s_f0), "launch_ms": round(bulk_ms, 4)},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
