@@ -15,9 +15,11 @@
 //
 // Work item: a 32 x 8 column of cells marching over `zchunk` z planes.  phi is
 // rebuilt from g on the fly (never re-read from DRAM) into a 5-plane ring with
-// a 2-cell halo; interface normals and |grad phi| live in a 3-plane ring with a
-// 1-cell halo; the populations of the cell are gathered straight from DRAM
-// (pull) and written back to the cell's own slots (aligned, coalesced).
+// a 2-cell halo; interface normals and |grad phi| live in a 2-plane ring with a
+// 1-cell halo; the curvature stencil is split into per-plane partial sums
+// that each thread carries along its own column in registers; the
+// populations of the cell are gathered straight from DRAM (pull) and written
+// back to the cell's own slots (aligned, coalesced).
 #pragma once
 
 #include "common.cuh"
@@ -66,12 +68,12 @@ struct Slab {
 struct BulkSmem {
     float phiR[5][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
     float phiZ[5][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
-    float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
+    float nrm[2][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field, slot = plane & 1
 };
 
 // Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
 __device__ __forceinline__ int ring5(int p) { return (int)((unsigned)(p + 10) % 5u); }
-__device__ __forceinline__ int ring3(int p) { return (int)((unsigned)(p + 9) % 3u); }
+__device__ __forceinline__ int ring2(int p) { return p & 1; }
 
 template <int Q, class TF, class TG>
 struct Bulk {
@@ -213,10 +215,15 @@ struct Bulk {
         __syncthreads();
         fill_nrm(S, zs - 1, tid);
         fill_nrm(S, zs, tid);
+        __syncthreads();
+        Curv cv;
+        cv.start(S, zs, tx, ty);
+        __syncthreads();
         for (int z = zs; z < ze; ++z) {
             fill_nrm(S, z + 1, tid);
             __syncthreads();
-            if (active) cell(a, S, x, y, z, tx, ty);
+            const float div = cv.advance(S, z, tx, ty);
+            if (active) cell(a, S, x, y, z, tx, ty, div);
             if (z + 1 < ze) fill_phi(a, S, x0, y0, z + 3, tid);
             __syncthreads();
         }
@@ -271,13 +278,14 @@ struct Bulk {
 
     // Normals and |grad phi| of plane pz over the tile + 1-cell halo.
     static __device__ void fill_nrm(BulkSmem &S, int pz, int tid) {
-        const int s = ring3(pz);
+        const int s = ring2(pz);
+        const int sm = ring5(pz - 1), s0 = ring5(pz), sp = ring5(pz + 1);
         for (int i = tid; i < kNX * kNY; i += kThreads) {
             const int nxh = i % kNX, nyh = i / kNX;
             float gx, gy, gz;
-            grad(S.phiZ, nxh + 1, nyh + 1, ring5(pz - 1), ring5(pz), ring5(pz + 1), gx, gy, gz);
+            grad(S.phiZ, nxh + 1, nyh + 1, sm, s0, sp, gx, gy, gz);
             const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
-            const float inv = 1.0f / (ind + 1e-9f);
+            const float inv = __frcp_rn(ind + 1e-9f); // = 1 / (ind + 1e-9), correctly rounded
             S.nrm[s][0][nyh][nxh] = gx * inv;
             S.nrm[s][1][nyh][nxh] = gy * inv;
             S.nrm[s][2][nyh][nxh] = gz * inv;
@@ -285,40 +293,84 @@ struct Bulk {
         }
     }
 
+    // Curvature by planes.  The divergence 3 sum_q w_q c_q . n(x + c_q)
+    // (phaseField.cuh:246-275) groups by c_qz: the plane of the cell itself
+    // contributes C, each neighbouring plane z +- 1 contributes S +- Z, where
+    // (dx, dy) runs over the 3 x 3 in-plane pattern of the velocity set:
+    //   C = w1 A + w2 B,  S = w2 A + w3 B,  Z = w1 nz + w2 (4 edge nz) + w3 (4 corner nz)
+    //   A = nx(+1, 0) - nx(-1, 0) + ny(0, +1) - ny(0, -1)
+    //   B = sum over the 4 corners (dx, dy) of dx nx + dy ny
+    // (w3 = 0 for D3Q19).  Every thread evaluates them once per plane for its
+    // own column and keeps the previous planes in registers, so the cell
+    // update reads 4 normal values instead of the full 3 x 3 x 3 stencil.
+    static __device__ __forceinline__ void plane_terms(const BulkSmem &S, int pz, int tx, int ty, float &C,
+                                                       float &Sv, float &Zv) {
+        const int s = ring2(pz);
+        const int cx = tx + 1, cy = ty + 1;
+        auto nx = [&](int dx, int dy) { return S.nrm[s][0][cy + dy][cx + dx]; };
+        auto ny = [&](int dx, int dy) { return S.nrm[s][1][cy + dy][cx + dx]; };
+        auto nz = [&](int dx, int dy) { return S.nrm[s][2][cy + dy][cx + dx]; };
+        const float A = (nx(1, 0) - nx(-1, 0)) + (ny(0, 1) - ny(0, -1));
+        const float B = ((nx(1, 1) - nx(-1, 1)) + (nx(1, -1) - nx(-1, -1))) +
+                        ((ny(1, 1) - ny(1, -1)) + (ny(-1, 1) - ny(-1, -1)));
+        const float E = (nz(1, 0) + nz(-1, 0)) + (nz(0, 1) + nz(0, -1));
+        C = fmaf(VS<Q>::w1, A, VS<Q>::w2 * B);
+        if constexpr (Q == 27) {
+            const float K = (nz(1, 1) + nz(-1, 1)) + (nz(1, -1) + nz(-1, -1));
+            Sv = fmaf(VS<Q>::w2, A, VS<Q>::w3 * B);
+            Zv = fmaf(VS<Q>::w1, nz(0, 0), fmaf(VS<Q>::w2, E, VS<Q>::w3 * K));
+        } else {
+            Sv = VS<Q>::w2 * A;
+            Zv = fmaf(VS<Q>::w1, nz(0, 0), VS<Q>::w2 * E);
+        }
+    }
+
+    // Per-thread curvature state along the column: C of the current plane and
+    // S - Z of the current and previous planes.
+    struct Curv {
+        float prev_d, cur_c, cur_d;
+        // planes zs - 1 and zs must be in the normal ring; ends before any
+        // thread may overwrite plane zs - 1 (the caller's next barrier)
+        __device__ __forceinline__ void start(const BulkSmem &S, int zs, int tx, int ty) {
+            float c, sv, zv;
+            plane_terms(S, zs - 1, tx, ty, c, sv, zv);
+            prev_d = sv - zv;
+            plane_terms(S, zs, tx, ty, cur_c, sv, zv);
+            cur_d = sv - zv;
+        }
+        // plane z + 1 just entered the ring: returns the divergence at plane z
+        __device__ __forceinline__ float advance(const BulkSmem &S, int z, int tx, int ty) {
+            float c, sv, zv;
+            plane_terms(S, z + 1, tx, ty, c, sv, zv);
+            const float div = cur_c + (sv + zv) + prev_d;
+            prev_d = cur_d;
+            cur_c = c;
+            cur_d = sv - zv;
+            return div;
+        }
+    };
+
     // Update of one fluid cell (x, y, z); (tx, ty) its position in the tile.
     // fs / gs: this plane's population slabs (slab path) or null (gather path).
     static __device__ __forceinline__ void cell(const A &a, const BulkSmem &S, int x, int y, int z,
-                                                int tx, int ty, const TF *fs = nullptr,
+                                                int tx, int ty, float div, const TF *fs = nullptr,
                                                 const TG *gs = nullptr) {
         const Geometry &G = a.geo;
         const Physics &P = a.phys;
         const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
         const uint32_t c0 = cell_index(G, x, y, z);
 
-        // ---- surface tension from the zeroed-ghost field (phaseField.cuh:246-293)
+        // ---- surface tension from the zeroed-ghost field (phaseField.cuh:246-293);
+        // div is the normal divergence of this cell, from the plane terms
         const int hx = tx + 2, hy = ty + 2; // phi ring centre
         const int nxh = tx + 1, nyh = ty + 1; // normal ring centre
-        const int sm = ring3(z - 1), s0 = ring3(z), sp = ring3(z + 1);
-        auto nat = [&](int comp, int dx, int dy, int dz) -> float {
-            const int sl = dz < 0 ? sm : (dz > 0 ? sp : s0);
-            return S.nrm[sl][comp][nyh + dy][nxh + dx];
-        };
-        float div = 0.f;
-        unroll<0, (Q - 1) / 2>([&](auto k) {
-            constexpr int q = 2 * k + 1;
-            constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
-            constexpr float w = (q <= 6) ? VS<Q>::w1 : (q <= 18 ? VS<Q>::w2 : VS<Q>::w3);
-            float d = 0.f;
-            if constexpr (cx != 0) d += float(cx) * (nat(0, cx, cy, cz) - nat(0, -cx, -cy, -cz));
-            if constexpr (cy != 0) d += float(cy) * (nat(1, cx, cy, cz) - nat(1, -cx, -cy, -cz));
-            if constexpr (cz != 0) d += float(cz) * (nat(2, cx, cy, cz) - nat(2, -cx, -cy, -cz));
-            div += w * d;
-        });
+        const int s0 = ring2(z);
+        auto nat = [&](int comp) -> float { return S.nrm[s0][comp][nyh][nxh]; };
         const float curvature = 3.0f * div;
-        const float stc = -P.sigma * curvature * nat(3, 0, 0, 0);
-        const float fx = stc * nat(0, 0, 0, 0);
-        const float fy = stc * nat(1, 0, 0, 0);
-        const float fz = stc * nat(2, 0, 0, 0);
+        const float stc = -P.sigma * curvature * nat(3);
+        const float fx = stc * nat(0);
+        const float fy = stc * nat(1);
+        const float fz = stc * nat(2);
 
         // ---- normals of the phase update from phi with ghost values (lbm.cu:157-224).
         // Away from ghost layers the raw and zeroed fields agree on the 3x3x3
@@ -326,12 +378,12 @@ struct Bulk {
         const bool near_ghost = (!px && (x <= G.x_lo || x >= G.x_hi)) ||
                                 (!py && (y <= G.y_lo || y >= G.y_hi)) ||
                                 (!pz && (z <= G.z_lo || z >= G.z_hi));
-        float nx = nat(0, 0, 0, 0), ny = nat(1, 0, 0, 0), nz = nat(2, 0, 0, 0);
+        float nx = nat(0), ny = nat(1), nz = nat(2);
         if (near_ghost) {
             float gx, gy, gz;
             grad(S.phiR, hx, hy, ring5(z - 1), ring5(z), ring5(z + 1), gx, gy, gz);
             const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
-            const float inv = 1.0f / (ind + 1e-9f);
+            const float inv = __frcp_rn(ind + 1e-9f);
             nx = gx * inv;
             ny = gy * inv;
             nz = gz * inv;
@@ -401,7 +453,7 @@ struct Bulk {
         // ---- hydrodynamics
         const Moments m = moments<Q>(f, fx, fy, fz);
         const float nu = fmaf(phi, P.nu_oil_minus_water, P.nu_water);
-        const float omega = 1.0f / (0.5f + 3.0f * nu);
+        const float omega = __frcp_rn(0.5f + 3.0f * nu); // = 1 / (...), correctly rounded
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
         unroll<0, Q>([&](auto q) { Store<TF>::st(a.f_dst + (uint64_t)q * N + c0, fo[q]); });
@@ -504,6 +556,10 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
         __syncthreads();
         B::fill_nrm(S, zs - 1, tid);
         B::fill_nrm(S, zs, tid);
+        __syncthreads();
+        typename B::Curv cv;
+        cv.start(S, zs, tx, ty);
+        __syncthreads();
         bool ok = true;
         for (int z = zs; z < ze; ++z) {
             const int k = z - zs;
@@ -519,7 +575,8 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
                 break;
             }
             mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs); // complete: visibility
-            if (active) B::cell(a, S, x, y, z, tx, ty, fstage(k), gstage(k));
+            const float div = cv.advance(S, z, tx, ty);
+            if (active) B::cell(a, S, x, y, z, tx, ty, div, fstage(k), gstage(k));
             if (z + 1 < ze) B::fill_phi(a, S, x0, y0, z + 3, tid);
             __syncthreads();
         }
@@ -583,6 +640,10 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
         if (ok) {
             B::fill_nrm(S, zs - 1, tid);
             B::fill_nrm(S, zs, tid);
+            __syncthreads();
+            typename B::Curv cv;
+            cv.start(S, zs, tx, ty);
+            __syncthreads();
             for (int z = zs; z < ze; ++z) {
                 B::fill_nrm(S, z + 1, tid);
                 const bool more = z + 1 < ze;
@@ -592,7 +653,8 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
                     ok = false;
                     break;
                 }
-                if (active) B::cell(a, S, x, y, z, tx, ty);
+                const float div = cv.advance(S, z, tx, ty);
+                if (active) B::cell(a, S, x, y, z, tx, ty, div);
                 if (more) B::fill_phi_box(a, S, confirm(z + 3), x0, y0, z + 3, tid);
                 __syncthreads();
                 if (more) issue(z + 5);

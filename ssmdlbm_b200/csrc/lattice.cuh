@@ -113,7 +113,7 @@ __device__ __forceinline__ Moments moments(const float (&f)[Q], float fx, float 
     });
     Moments m;
     m.rho = s + 1.0f;
-    const float inv = 1.0f / m.rho;
+    const float inv = __frcp_rn(m.rho); // = 1 / rho, correctly rounded
     const float hinv = 0.5f * inv;
     m.ux = jx * inv + fx * hinv;
     m.uy = jy * inv + fy * hinv;
