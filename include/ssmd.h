@@ -76,6 +76,17 @@ typedef struct CUgraphExec_st *ssmd_graph_exec_t;
 /* ------------------------------------------------------------ step flags */
 #define SSMD_STEP_STORE_MACROS 1u /* write rho, ux, uy, uz, phi at every cell */
 
+/* Closure network: 12 features -> 64 -> 64 -> 2, GELU.  A network is one FP32
+ * device buffer of SSMD_MLP_NET_FLOATS: the SSMD_MLP_PARAMS trainable values
+ * W1 [64][16] (input columns 12..15 zero), b1 [64], W2 [64][64], b2 [64],
+ * W3 [2][64], b3 [2], then feature mean [12], feature 1/std [12], output
+ * scale [2] and output offset [2]. */
+#define SSMD_MLP_IN 12
+#define SSMD_MLP_HIDDEN 64
+#define SSMD_MLP_OUT 2
+#define SSMD_MLP_PARAMS 5378
+#define SSMD_MLP_NET_FLOATS 5406
+
 /*
  * Field container.  Member order and meaning are those of the reference's
  * struct LBMFields (src/structs/LBMFields.cuh:26-49) so code that reads
@@ -151,8 +162,35 @@ typedef struct ssmd_params {
 
     int32_t tile_z;   /* z planes per bulk work item (0: library default)     */
     int32_t bulk_path; /* SSMD_PATH_*: how the bulk kernel feeds the phi halo */
-    int32_t reserved[6];
+    const struct ssmd_derived *derived; /* derived-field arrays (NULL: none)   */
+    const struct ssmd_closure *closure; /* per-cell closure arrays read by the
+                                           bulk kernel (NULL: plain method)    */
+    int32_t reserved[2];
 } ssmd_params;
+
+/*
+ * Derived fields (reference src/derivedFields/DerivedFields.cuh:39-58 and
+ * LBMFields.cuh:51-84): FP32 arrays of nx*ny*nz cells, each may be NULL.
+ * Running means follow timeAverage.cuh:58-61 / reynoldsMoments.cuh:58-61,
+ * avg <- avg + (value - avg) / t with t the 1-based index of the step just
+ * completed; vorticity follows vorticityFields.cuh:37-96.
+ */
+typedef struct ssmd_derived {
+    float *avg_phi, *avg_ux, *avg_uy, *avg_uz;
+    float *avg_uxux, *avg_uyuy, *avg_uzuz, *avg_uxuy, *avg_uxuz, *avg_uyuz;
+    float *vort_x, *vort_y, *vort_z, *vort_mag;
+} ssmd_derived;
+
+/*
+ * Learned closure state of a (coarse) lattice: per-cell eddy viscosity added
+ * to nu(phi) and a factor on the surface tension, both FP32 nx*ny*nz arrays
+ * written by ssmd_closure_apply and read by the bulk kernel.  No reference
+ * counterpart: the reference runs the plain method only.
+ */
+typedef struct ssmd_closure {
+    const float *nut;         /* eddy viscosity (lattice units), >= 0          */
+    const float *sigma_scale; /* factor on sigma at the cell                   */
+} ssmd_closure;
 
 /* Global reductions, accumulated in FP64 over the fluid (non-ghost) cells. */
 typedef struct ssmd_stats {
@@ -368,6 +406,46 @@ int ssmd_output_info(const char *dir, const char *id, const char *velocity_set, 
 /* Reads and clears the device status word (synchronises the stream):
  * bit 0 = a bulk cell produced a non-finite density. */
 int ssmd_check_status(const ssmd_params *p, uint32_t *status_out, ssmd_stream_t stream);
+
+/*
+ * Learned closure (no reference counterpart).  The network runs on the
+ * tcgen05 tensor cores, 128 cells per CTA, bf16 operands, FP32 accumulation.
+ *   ssmd_mlp_forward: out[i][0..1] = scale * net(features[i]) + offset.
+ *   ssmd_mlp_grad: overwrites grad (SSMD_MLP_PARAMS floats) with dL/dparams
+ *     and *loss (device double) with L = (1/n) sum_i sum_k w_ik (r_ik -
+ *     (t_ik - offset_k)/scale_k)^2, r the raw output; weights may be NULL (1).
+ *   ssmd_mlp_adam: one Adam step (bias-corrected, step t >= 1) on the params.
+ *   ssmd_mlp_status: bit 0 set when an MMA wait timed out (the CTA aborted).
+ * Features (ssmd_closure_features), per cell, from rho, ux, uy, uz, phi with
+ * central differences (periodic axes wrap, others clamp at the faces):
+ *   phi, 4 phi (1 - phi), |grad phi|, laplacian phi, |S| = sqrt(2 S:S),
+ *   |curl u|, n.S.n (n = grad phi / |grad phi|), |u|, u_z, rho - 1, div u,
+ *   nu(phi).
+ * ssmd_closure_filter box-filters a fine lattice 2x (even sizes) into coarse
+ * rho, ux, uy, uz, phi (5 arrays of the coarse cell count, in that order),
+ * the subgrid stress tau_ij = <u_i u_j> - <u_i><u_j> (6 arrays: xx, yy, zz,
+ * xy, xz, yz) and the mean fine |grad phi| (1 array).  ssmd_closure_targets
+ * turns them into training targets on the coarse lattice: nu_t* =
+ * clamp(-tau^d : S / (2 S:S + 1e-12), 0, nut_max) and sigma* = the ratio of
+ * the fine interface area density to the coarse one, 2 <|grad phi|> /
+ * |grad phi_c|, clamped to [0.25, 4] (1 where |grad phi_c| < 1e-2), with
+ * weights 1 and 4 phi (1 - phi) + 0.01.  ssmd_closure_apply evaluates the
+ * network on features and writes nut = clamp(out0, 0, nut_max) and
+ * sigma_scale = clamp(out1, 0.25, 4); out is 2 * cells floats of scratch.
+ */
+int ssmd_mlp_forward(const float *net, const float *features, int64_t n, float *out, ssmd_stream_t stream);
+int ssmd_mlp_grad(const float *net, const float *features, const float *targets, const float *weights, int64_t n,
+                  float *grad, double *loss, ssmd_stream_t stream);
+int ssmd_mlp_adam(float *net, const float *grad, float *m, float *v, int64_t t, float lr, float beta1,
+                  float beta2, float eps, ssmd_stream_t stream);
+int ssmd_mlp_status(uint32_t *status);
+int ssmd_closure_features(const ssmd_params *p, const LBMFields *fields, float *features, ssmd_stream_t stream);
+int ssmd_closure_filter(const ssmd_params *fine, const LBMFields *fine_fields, float *coarse, float *tau,
+                        float *area, ssmd_stream_t stream);
+int ssmd_closure_targets(const ssmd_params *coarse, const float *coarse_fields, const float *tau,
+                         const float *area, float nut_max, float *targets, float *weights, ssmd_stream_t stream);
+int ssmd_closure_apply(const ssmd_params *coarse, const float *net, const float *features, float *out,
+                       float *nut, float *sigma_scale, float nut_max, ssmd_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -54,7 +54,8 @@ class Params(ctypes.Structure):
         ("u_water", c_float), ("water_cx", c_float), ("water_cz", c_float), ("water_r2", c_float),
         ("noise_amp", c_float), ("u_limit", c_float), ("seed", c_uint64),
         ("f_alt", c_void_p), ("g_alt", c_void_p), ("workspace", c_void_p), ("workspace_bytes", c_size_t),
-        ("tile_z", c_int32), ("bulk_path", c_int32), ("reserved", c_int32 * 6),
+        ("tile_z", c_int32), ("bulk_path", c_int32),
+        ("derived", c_void_p), ("closure", c_void_p), ("reserved", c_int32 * 2),
     ]
 
     def copy(self) -> "Params":
@@ -81,6 +82,23 @@ class Stats(ctypes.Structure):
 class Droplet(ctypes.Structure):
     _fields_ = [("root", c_uint32), ("cells", c_uint32), ("volume", c_double), ("touches_inlet", c_uint32),
                 ("reserved", c_uint32)]
+
+
+class Derived(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in (
+        "avg_phi", "avg_ux", "avg_uy", "avg_uz", "avg_uxux", "avg_uyuy", "avg_uzuz", "avg_uxuy", "avg_uxuz",
+        "avg_uyuz", "vort_x", "vort_y", "vort_z", "vort_mag")]
+
+
+class Closure(ctypes.Structure):
+    _fields_ = [("nut", c_void_p), ("sigma_scale", c_void_p)]
+
+
+MLP_IN = 12
+MLP_HIDDEN = 64
+MLP_OUT = 2
+MLP_PARAMS = 5378
+MLP_NET_FLOATS = 5406
 
 
 class SSMDError(RuntimeError):
@@ -136,6 +154,19 @@ SIGNATURES = [
     ("ssmd_profile_enable", c_int32, [c_int32]),
     ("ssmd_profile_read", c_int32, [POINTER(c_float), c_int32, POINTER(c_int32)]),
     ("ssmd_profile_disable", c_int32, []),
+    ("ssmd_mlp_forward", c_int32, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
+    ("ssmd_mlp_grad", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,
+                                c_void_p]),
+    ("ssmd_mlp_adam", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_float, c_float,
+                                c_float, c_float, c_void_p]),
+    ("ssmd_mlp_status", c_int32, [POINTER(c_uint32)]),
+    ("ssmd_closure_features", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_void_p]),
+    ("ssmd_closure_filter", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_void_p, c_void_p,
+                                      c_void_p]),
+    ("ssmd_closure_targets", c_int32, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_float, c_void_p,
+                                       c_void_p, c_void_p]),
+    ("ssmd_closure_apply", c_int32, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_float, c_void_p]),
 ]
 
 

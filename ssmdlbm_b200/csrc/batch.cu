@@ -75,6 +75,7 @@ int prepare(const ssmd_params *params, const LBMFields *fields, int32_t count, v
             a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
             a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
             a.status = status_of(p);
+            set_closure(a, p);
             a.flags = 0;
             // batch items: a fixed z chunk (tile_z, default 16) keeps items of
             // different lattices comparable in work

@@ -367,7 +367,8 @@ struct Bulk {
         const int s0 = ring2(z);
         auto nat = [&](int comp) -> float { return S.nrm[s0][comp][nyh][nxh]; };
         const float curvature = 3.0f * div;
-        const float stc = -P.sigma * curvature * nat(3);
+        const float sigma = a.clo_cs ? P.sigma * a.clo_cs[c0] : P.sigma;
+        const float stc = -sigma * curvature * nat(3);
         const float fx = stc * nat(0);
         const float fy = stc * nat(1);
         const float fz = stc * nat(2);
@@ -452,7 +453,8 @@ struct Bulk {
 
         // ---- hydrodynamics
         const Moments m = moments<Q>(f, fx, fy, fz);
-        const float nu = fmaf(phi, P.nu_oil_minus_water, P.nu_water);
+        float nu = fmaf(phi, P.nu_oil_minus_water, P.nu_water);
+        if (a.clo_nut) nu += a.clo_nut[c0];
         const float omega = __frcp_rn(0.5f + 3.0f * nu); // = 1 / (...), correctly rounded
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);

@@ -1,0 +1,246 @@
+// closure.cu — features, training targets and application of the learned closure.
+//
+// The closure runs the plain method on a 2x coarser lattice and corrects it
+// per cell: an eddy viscosity nu_t added to nu(phi), and a factor on the
+// surface tension.  Training data come from the solver's own fine runs:
+// ssmd_closure_filter box-filters a fine lattice onto the coarse one (the
+// resolved fields, the subgrid stress and the fine interface area density),
+// ssmd_closure_targets turns them into the two targets, and
+// ssmd_closure_features computes the network inputs from any lattice's
+// macroscopic fields, so filtered fine data and a live coarse run are
+// described by the same numbers.  Derivatives are central differences;
+// exact-periodic axes wrap, the others clamp at the faces.
+#include <cuda_runtime.h>
+
+#include "host.cuh"
+
+using namespace ssmd;
+using namespace ssmd::host;
+
+namespace {
+
+struct Grid {
+    int nx, ny, nz;
+    bool px, py, pz;
+};
+
+Grid grid_of(const ssmd_params &p) {
+    return Grid{(int)p.nx, (int)p.ny, (int)p.nz, p.bc_x == SSMD_BC_PERIODIC, p.bc_y == SSMD_BC_PERIODIC,
+                p.bc_z == SSMD_BC_PERIODIC};
+}
+
+__device__ __forceinline__ int nbr(int c, int d, int n, bool per) {
+    int v = c + d;
+    if (per) v = v < 0 ? v + n : (v >= n ? v - n : v);
+    else v = v < 0 ? 0 : (v >= n ? n - 1 : v);
+    return v;
+}
+
+__device__ __forceinline__ int64_t idx(const Grid &g, int x, int y, int z) {
+    return (int64_t)x + (int64_t)g.nx * ((int64_t)y + (int64_t)g.ny * z);
+}
+
+// Central-difference gradient of a scalar array at (x, y, z).
+__device__ __forceinline__ void grad3(const Grid &g, const float *a, int x, int y, int z, float &gx, float &gy,
+                                      float &gz) {
+    gx = 0.5f * (a[idx(g, nbr(x, 1, g.nx, g.px), y, z)] - a[idx(g, nbr(x, -1, g.nx, g.px), y, z)]);
+    gy = 0.5f * (a[idx(g, x, nbr(y, 1, g.ny, g.py), z)] - a[idx(g, x, nbr(y, -1, g.ny, g.py), z)]);
+    gz = 0.5f * (a[idx(g, x, y, nbr(z, 1, g.nz, g.pz))] - a[idx(g, x, y, nbr(z, -1, g.nz, g.pz))]);
+}
+
+// Velocity gradient d[i][j] = d u_i / d x_j and the strain rate S = (d + d^T)/2.
+__device__ __forceinline__ void strain(const Grid &g, const float *ux, const float *uy, const float *uz, int x,
+                                       int y, int z, float (&d)[3][3]) {
+    grad3(g, ux, x, y, z, d[0][0], d[0][1], d[0][2]);
+    grad3(g, uy, x, y, z, d[1][0], d[1][1], d[1][2]);
+    grad3(g, uz, x, y, z, d[2][0], d[2][1], d[2][2]);
+}
+
+__global__ void features_kernel(Grid g, const float *rho, const float *ux, const float *uy, const float *uz,
+                                const float *phi, float nu_w, float nu_dow, float *feat) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+    if (i >= cells) return;
+    const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((int64_t)g.nx * g.ny));
+    const float ph = phi[i];
+    float gx, gy, gz;
+    grad3(g, phi, x, y, z, gx, gy, gz);
+    const float gmag = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float lap = phi[idx(g, nbr(x, 1, g.nx, g.px), y, z)] + phi[idx(g, nbr(x, -1, g.nx, g.px), y, z)] +
+                      phi[idx(g, x, nbr(y, 1, g.ny, g.py), z)] + phi[idx(g, x, nbr(y, -1, g.ny, g.py), z)] +
+                      phi[idx(g, x, y, nbr(z, 1, g.nz, g.pz))] + phi[idx(g, x, y, nbr(z, -1, g.nz, g.pz))] -
+                      6.0f * ph;
+    float d[3][3];
+    strain(g, ux, uy, uz, x, y, z, d);
+    float ss = 0.f, nsn = 0.f;
+    const float inv = 1.0f / (gmag + 1e-9f);
+    const float n[3] = {gx * inv, gy * inv, gz * inv};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const float s = 0.5f * (d[a][b] + d[b][a]);
+            ss += s * s;
+            nsn += n[a] * s * n[b];
+        }
+    const float wx = d[2][1] - d[1][2], wy = d[0][2] - d[2][0], wz = d[1][0] - d[0][1];
+    const float u0 = ux[i], u1 = uy[i], u2 = uz[i];
+    float *f = feat + i * SSMD_MLP_IN;
+    f[0] = ph;
+    f[1] = 4.0f * ph * (1.0f - ph);
+    f[2] = gmag;
+    f[3] = lap;
+    f[4] = sqrtf(2.0f * ss);
+    f[5] = sqrtf(wx * wx + wy * wy + wz * wz);
+    f[6] = nsn;
+    f[7] = sqrtf(u0 * u0 + u1 * u1 + u2 * u2);
+    f[8] = u2;
+    f[9] = rho[i] - 1.0f;
+    f[10] = d[0][0] + d[1][1] + d[2][2];
+    f[11] = fmaf(ph, nu_dow, nu_w);
+}
+
+// One thread per coarse cell: means over the 2 x 2 x 2 fine block.
+__global__ void filter_kernel(Grid fg, Grid cg, const float *rho, const float *ux, const float *uy, const float *uz,
+                              const float *phi, float *coarse, float *tau, float *area) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cells = (int64_t)cg.nx * cg.ny * cg.nz;
+    if (i >= cells) return;
+    const int X = (int)(i % cg.nx), Y = (int)((i / cg.nx) % cg.ny), Z = (int)(i / ((int64_t)cg.nx * cg.ny));
+    double m[5] = {0, 0, 0, 0, 0}, uu[6] = {0, 0, 0, 0, 0, 0}, a = 0.0;
+    for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < 2; ++j)
+            for (int l = 0; l < 2; ++l) {
+                const int x = 2 * X + l, y = 2 * Y + j, z = 2 * Z + k;
+                const int64_t c = idx(fg, x, y, z);
+                const float u0 = ux[c], u1 = uy[c], u2 = uz[c];
+                m[0] += rho[c];
+                m[1] += u0;
+                m[2] += u1;
+                m[3] += u2;
+                m[4] += phi[c];
+                uu[0] += (double)u0 * u0;
+                uu[1] += (double)u1 * u1;
+                uu[2] += (double)u2 * u2;
+                uu[3] += (double)u0 * u1;
+                uu[4] += (double)u0 * u2;
+                uu[5] += (double)u1 * u2;
+                float gx, gy, gz;
+                grad3(fg, phi, x, y, z, gx, gy, gz);
+                a += sqrt((double)gx * gx + (double)gy * gy + (double)gz * gz);
+            }
+    for (int q = 0; q < 5; ++q) m[q] *= 0.125;
+    for (int q = 0; q < 6; ++q) uu[q] *= 0.125;
+    for (int q = 0; q < 5; ++q) coarse[q * cells + i] = (float)m[q];
+    tau[0 * cells + i] = (float)(uu[0] - m[1] * m[1]);
+    tau[1 * cells + i] = (float)(uu[1] - m[2] * m[2]);
+    tau[2 * cells + i] = (float)(uu[2] - m[3] * m[3]);
+    tau[3 * cells + i] = (float)(uu[3] - m[1] * m[2]);
+    tau[4 * cells + i] = (float)(uu[4] - m[1] * m[3]);
+    tau[5 * cells + i] = (float)(uu[5] - m[2] * m[3]);
+    area[i] = (float)(0.125 * a);
+}
+
+__global__ void targets_kernel(Grid g, const float *cf, const float *tau, const float *area, float nut_max,
+                               float *targets, float *weights) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+    if (i >= cells) return;
+    const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((int64_t)g.nx * g.ny));
+    const float *ux = cf + 1 * cells, *uy = cf + 2 * cells, *uz = cf + 3 * cells, *phi = cf + 4 * cells;
+    float d[3][3];
+    strain(g, ux, uy, uz, x, y, z, d);
+    const float t[3][3] = {{tau[0 * cells + i], tau[3 * cells + i], tau[4 * cells + i]},
+                           {tau[3 * cells + i], tau[1 * cells + i], tau[5 * cells + i]},
+                           {tau[4 * cells + i], tau[5 * cells + i], tau[2 * cells + i]}};
+    const float tr = (t[0][0] + t[1][1] + t[2][2]) * (1.0f / 3.0f);
+    float num = 0.f, den = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const float s = 0.5f * (d[a][b] + d[b][a]);
+            num += (t[a][b] - (a == b ? tr : 0.f)) * s;
+            den += s * s;
+        }
+    const float nut = fminf(fmaxf(-num / (2.0f * den + 1e-12f), 0.0f), nut_max);
+    float gx, gy, gz;
+    grad3(g, phi, x, y, z, gx, gy, gz);
+    const float gm = sqrtf(gx * gx + gy * gy + gz * gz);
+    float cs = 1.0f;
+    if (gm >= 1e-2f) cs = fminf(fmaxf(2.0f * area[i] / gm, 0.25f), 4.0f);
+    const float ph = phi[i];
+    targets[2 * i + 0] = nut;
+    targets[2 * i + 1] = cs;
+    weights[2 * i + 0] = 1.0f;
+    weights[2 * i + 1] = 4.0f * ph * (1.0f - ph) + 0.01f;
+}
+
+__global__ void apply_kernel(int64_t cells, const float *out, float nut_max, float *nut, float *cs) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= cells) return;
+    nut[i] = fminf(fmaxf(out[2 * i + 0], 0.0f), nut_max);
+    cs[i] = fminf(fmaxf(out[2 * i + 1], 0.25f), 4.0f);
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned)((n + 255) / 256); }
+
+} // namespace
+
+extern "C" int ssmd_closure_features(const ssmd_params *p, const LBMFields *fields, float *features,
+                                     ssmd_stream_t stream) {
+    if (int e = ssmd_validate(p)) return e;
+    if (!fields || !fields->rho || !fields->ux || !fields->uy || !fields->uz || !fields->phi || !features)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    const Grid g = grid_of(*p);
+    const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+    features_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        g, fields->rho, fields->ux, fields->uy, fields->uz, fields->phi, p->nu_water, p->nu_oil - p->nu_water,
+        features);
+    return cuda_check(cudaGetLastError(), "features launch");
+}
+
+extern "C" int ssmd_closure_filter(const ssmd_params *fine, const LBMFields *fine_fields, float *coarse, float *tau,
+                                   float *area, ssmd_stream_t stream) {
+    if (int e = ssmd_validate(fine)) return e;
+    if (!fine_fields || !fine_fields->rho || !fine_fields->ux || !fine_fields->uy || !fine_fields->uz ||
+        !fine_fields->phi || !coarse || !tau || !area)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    if ((fine->nx | fine->ny | fine->nz) & 1u)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "filtering needs even lattice sizes (%u x %u x %u)", fine->nx,
+                    fine->ny, fine->nz);
+    const Grid fg = grid_of(*fine);
+    Grid cg = fg;
+    cg.nx /= 2;
+    cg.ny /= 2;
+    cg.nz /= 2;
+    const int64_t cells = (int64_t)cg.nx * cg.ny * cg.nz;
+    filter_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        fg, cg, fine_fields->rho, fine_fields->ux, fine_fields->uy, fine_fields->uz, fine_fields->phi, coarse, tau,
+        area);
+    return cuda_check(cudaGetLastError(), "filter launch");
+}
+
+extern "C" int ssmd_closure_targets(const ssmd_params *coarse, const float *coarse_fields, const float *tau,
+                                    const float *area, float nut_max, float *targets, float *weights,
+                                    ssmd_stream_t stream) {
+    if (int e = ssmd_validate(coarse)) return e;
+    if (!coarse_fields || !tau || !area || !targets || !weights)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    const Grid g = grid_of(*coarse);
+    const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+    targets_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        g, coarse_fields, tau, area, nut_max, targets, weights);
+    return cuda_check(cudaGetLastError(), "targets launch");
+}
+
+extern "C" int ssmd_closure_apply(const ssmd_params *coarse, const float *net, const float *features, float *out,
+                                  float *nut, float *sigma_scale, float nut_max, ssmd_stream_t stream) {
+    if (int e = ssmd_validate(coarse)) return e;
+    if (!net || !features || !out || !nut || !sigma_scale) return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    const int64_t cells = (int64_t)coarse->nx * coarse->ny * coarse->nz;
+    if (int e = ssmd_mlp_forward(net, features, cells, out, stream)) return e;
+    apply_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(cells, out, nut_max, nut,
+                                                                                        sigma_scale);
+    return cuda_check(cudaGetLastError(), "closure apply launch");
+}

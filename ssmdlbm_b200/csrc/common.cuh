@@ -82,6 +82,8 @@ struct StepArgs {
     const TG *__restrict__ g_src;
     TG *__restrict__ g_dst;
     DeviceStatus *status;
+    const float *clo_nut; // learned closure: eddy viscosity per cell (null: off)
+    const float *clo_cs;  // learned closure: surface-tension factor per cell
     uint32_t flags;       // SSMD_STEP_*
     int tiles_x, tiles_y; // bulk tiling
     int zchunk, nzchunks;

@@ -171,6 +171,12 @@ inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tile
     nchunks = (nzf + zchunk - 1) / zchunk;
 }
 
+template <class TF, class TG>
+inline void set_closure(StepArgs<TF, TG> &a, const ssmd_params &p) {
+    a.clo_nut = p.closure ? p.closure->nut : nullptr;
+    a.clo_cs = (p.closure && p.closure->nut) ? p.closure->sigma_scale : nullptr;
+}
+
 template <int Q, class T>
 int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32_t flags,
                 cudaStream_t st) {
@@ -184,6 +190,7 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
     a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
     a.status = status_of(p);
+    set_closure(a, p);
     a.flags = flags;
     // Kernel path: per-cell gathers (default), TMA boxes for the phi halo, or
     // TMA slabs for the populations; the TMA paths need a 16-byte aligned x pitch.

@@ -1,0 +1,225 @@
+"""Learned closure on the GPU: the tcgen05 network, its gradient and Adam
+against the CPU oracle, the data kernels against numpy, and the coupling of
+the closure arrays into the step."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from ssmdlbm_b200 import _lib, configs
+from ssmdlbm_b200._lib import check, lib
+from oracle import closure_oracle as co
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def _net(seed):
+    rng = np.random.default_rng(seed)
+    net = co.init_net(seed)
+    net[co.oB1:co.oW2] = rng.normal(0, 0.1, co.HID)
+    net[co.oB2:co.oW3] = rng.normal(0, 0.1, co.HID)
+    net[co.oB3:co.PARAMS] = rng.normal(0, 0.1, co.OUT)
+    net[co.oMean:co.oInvStd] = rng.normal(0, 0.5, co.IN)
+    net[co.oInvStd:co.oScale] = rng.uniform(0.5, 2.0, co.IN)
+    net[co.oScale:co.oOffset] = [0.01, 2.0]
+    net[co.oOffset:co.NET] = [0.0, 1.0]
+    return net
+
+
+def _status():
+    s = ctypes.c_uint32()
+    check(lib().ssmd_mlp_status(ctypes.byref(s)))
+    return s.value
+
+
+def test_forward_matches_oracle():
+    rng = np.random.default_rng(0)
+    n = 1000  # not a multiple of 128: the last CTA is partly empty
+    net = _net(1)
+    feat = rng.normal(0, 1.5, (n, co.IN)).astype(np.float32)
+    out = torch.empty(n, 2, device="cuda")
+    dn, df = _dev(net), _dev(feat)  # kept alive across the asynchronous call
+    check(lib().ssmd_mlp_forward(dn.data_ptr(), df.data_ptr(), n, out.data_ptr(), None))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().astype(np.float64)
+    ref = co.predict(net, feat)
+    for k in range(2):
+        err = np.abs(got[:, k] - ref[:, k])
+        scale = np.abs(ref[:, k]).max()
+        # bf16 operands: a hidden activation that rounds the other way moves the
+        # output by ~2^-9 of its contribution
+        assert err.max() <= 1e-2 * scale, (k, err.max(), scale)
+        assert np.median(err) <= 1e-3 * scale
+    assert _status() == 0
+
+
+def test_gradient_matches_oracle():
+    rng = np.random.default_rng(1)
+    n = 700
+    net = _net(2)
+    feat = rng.normal(0, 1.5, (n, co.IN)).astype(np.float32)
+    tgt = np.stack([rng.uniform(0, 0.02, n), rng.uniform(0.5, 2, n)], 1).astype(np.float32)
+    w = rng.uniform(0.1, 1.0, (n, 2)).astype(np.float32)
+    grad = torch.empty(co.PARAMS, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    dn, df, dt, dw = _dev(net), _dev(feat), _dev(tgt), _dev(w)
+    check(lib().ssmd_mlp_grad(dn.data_ptr(), df.data_ptr(), dt.data_ptr(), dw.data_ptr(), n, grad.data_ptr(),
+                              loss.data_ptr(), None))
+    torch.cuda.synchronize()
+    g = grad.cpu().numpy().astype(np.float64)
+    l_ref, g_ref = co.loss_and_grad(net, feat, tgt, w)
+    assert abs(loss.item() - l_ref) <= 1e-3 * l_ref
+    rel = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    cos = g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref))
+    assert rel <= 1e-2 and cos >= 0.9999, (rel, cos)
+    for a, b in ((co.oW1, co.oB1), (co.oB1, co.oW2), (co.oW2, co.oB2), (co.oB2, co.oW3), (co.oW3, co.oB3),
+                 (co.oB3, co.PARAMS)):
+        r = np.linalg.norm(g[a:b] - g_ref[a:b]) / max(np.linalg.norm(g_ref[a:b]), 1e-30)
+        assert r <= 2e-2, (a, b, r)
+    assert np.all(g[co.oW1:co.oB1].reshape(co.HID, co.K1)[:, co.IN:] == 0)
+    assert _status() == 0
+
+
+def test_adam_matches_oracle():
+    rng = np.random.default_rng(2)
+    net = _net(3)
+    g = rng.normal(0, 1e-2, co.PARAMS).astype(np.float32)
+    m = rng.normal(0, 1e-3, co.PARAMS).astype(np.float32)
+    v = rng.uniform(0, 1e-4, co.PARAMS).astype(np.float32)
+    dn, dm, dv, dg = _dev(net), _dev(m), _dev(v), _dev(g)
+    check(lib().ssmd_mlp_adam(dn.data_ptr(), dg.data_ptr(), dm.data_ptr(), dv.data_ptr(), 7, 1e-3, 0.9, 0.999,
+                              1e-8, None))
+    torch.cuda.synchronize()
+    rn, rm, rv = co.adam(net, g.astype(np.float64), m, v, 7, 1e-3)
+    assert np.allclose(dn.cpu().numpy(), rn, rtol=1e-5, atol=1e-7)
+    assert np.allclose(dm.cpu().numpy(), rm, rtol=1e-5, atol=1e-9)  # fp32 ulp of |m| ~ 1e-3: 1.2e-10
+    assert np.allclose(dv.cpu().numpy(), rv, rtol=1e-5, atol=1e-11)
+    assert np.array_equal(dn.cpu().numpy()[co.PARAMS:], net[co.PARAMS:])
+
+
+def test_training_reduces_loss():
+    rng = np.random.default_rng(4)
+    n = 4096
+    feat = rng.normal(0, 1, (n, co.IN)).astype(np.float32)
+    tgt = np.stack([0.01 * np.tanh(feat[:, 0] * feat[:, 1]) + 0.01, 1.0 + 0.5 * np.sin(feat[:, 2])], 1)
+    tgt = tgt.astype(np.float32)
+    net = co.init_net(5)
+    net[co.oScale:co.oOffset] = [0.01, 0.5]
+    net[co.oOffset:co.NET] = [0.01, 1.0]
+    dn = _dev(net)
+    m = torch.zeros(co.PARAMS, device="cuda")
+    v = torch.zeros(co.PARAMS, device="cuda")
+    grad = torch.empty(co.PARAMS, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    df, dt = _dev(feat), _dev(tgt)
+    L = lib()
+    losses = []
+    for t in range(1, 401):
+        check(L.ssmd_mlp_grad(dn.data_ptr(), df.data_ptr(), dt.data_ptr(), None, n, grad.data_ptr(),
+                              loss.data_ptr(), None))
+        check(L.ssmd_mlp_adam(dn.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), t, 3e-3, 0.9, 0.999,
+                              1e-8, None))
+        if t in (1, 400):
+            losses.append(loss.item())
+    assert losses[1] < 0.1 * losses[0], losses
+    assert _status() == 0
+
+
+def _jet_fields(shape=(16, 16, 32), steps=30):
+    from ssmdlbm_b200.lbm import Simulation
+    p = configs.oil_jet(*shape, 19, tau=0.55, sigma=1e-3, mobility=0.1, diam=6, w_in=0.05, noise=0.01, seed=3)
+    s = Simulation(p)
+    s.init()
+    s.step(steps, store_macros=True)
+    s.sync()
+    return p, s
+
+
+def test_features_filter_targets_match_oracle():
+    p, s = _jet_fields()
+    L = lib()
+    per = (True, True, False)
+    fields = {k: s.field(k) for k in ("rho", "ux", "uy", "uz", "phi")}
+    n = s.cells
+    feat = torch.empty(n, 12, device="cuda")
+    check(L.ssmd_closure_features(ctypes.byref(s.p), ctypes.byref(s.fields), feat.data_ptr(), s.stream))
+    s.sync()
+    ref = co.features(fields["rho"], fields["ux"], fields["uy"], fields["uz"], fields["phi"], per,
+                      float(s.p.nu_water), float(s.p.nu_oil))
+    got = feat.cpu().numpy()
+    for k in range(12):
+        sc = max(np.abs(ref[:, k]).max(), 1e-12)
+        assert np.abs(got[:, k] - ref[:, k]).max() <= 2e-5 * sc, k
+    # 2x filter onto the coarse lattice, then targets there
+    nc = n // 8
+    coarse = torch.empty(5 * nc, device="cuda")
+    tau = torch.empty(6 * nc, device="cuda")
+    area = torch.empty(nc, device="cuda")
+    check(L.ssmd_closure_filter(ctypes.byref(s.p), ctypes.byref(s.fields), coarse.data_ptr(), tau.data_ptr(),
+                                area.data_ptr(), s.stream))
+    s.sync()
+    rc, rt, ra = co.box_filter(fields["rho"], fields["ux"], fields["uy"], fields["uz"], fields["phi"], per)
+    cshape = rc[0].shape
+    got_c = coarse.cpu().numpy().reshape(5, *cshape)
+    for q in range(5):
+        assert np.allclose(got_c[q], rc[q], rtol=1e-6, atol=1e-7), q
+    got_t = tau.cpu().numpy().reshape(6, *cshape)
+    for q in range(6):
+        assert np.allclose(got_t[q], rt[q], rtol=1e-4, atol=1e-10), q
+    assert np.allclose(area.cpu().numpy().reshape(cshape), ra, rtol=1e-5, atol=1e-7)
+    cp = configs.oil_jet(cshape[2], cshape[1], cshape[0], 19, tau=0.55, sigma=1e-3, mobility=0.1, diam=3)
+    tg = torch.empty(nc, 2, device="cuda")
+    wt = torch.empty(nc, 2, device="cuda")
+    check(L.ssmd_closure_targets(ctypes.byref(cp), coarse.data_ptr(), tau.data_ptr(), area.data_ptr(), 0.05,
+                                 tg.data_ptr(), wt.data_ptr(), None))
+    torch.cuda.synchronize()
+    rtg, rw = co.targets([got_c[q] for q in range(5)], [got_t[q] for q in range(6)], area.cpu().numpy().reshape(cshape),
+                         per, 0.05)
+    assert np.allclose(tg.cpu().numpy()[:, 0], rtg[:, 0], rtol=1e-3, atol=1e-7)
+    assert np.allclose(tg.cpu().numpy()[:, 1], rtg[:, 1], rtol=1e-4, atol=1e-5)
+    assert np.allclose(wt.cpu().numpy(), rw, rtol=1e-6, atol=1e-7)
+    s.close()
+
+
+def _closure_run(nut_value, cs_value, steps=20):
+    from ssmdlbm_b200.lbm import Simulation
+    p = configs.oil_jet(24, 24, 48, 19, tau=0.55, sigma=5e-3, mobility=0.1, diam=8, w_in=0.05, noise=0.01, seed=4)
+    s = Simulation(p)
+    keep = None
+    if nut_value is not None:
+        nut = torch.full((s.cells,), nut_value, device="cuda")
+        cs = torch.full((s.cells,), cs_value, device="cuda")
+        cl = _lib.Closure(nut.data_ptr(), cs.data_ptr())
+        s.p.closure = ctypes.addressof(cl)
+        keep = (nut, cs, cl)
+    s.init()
+    s.step(steps, store_macros=True)
+    out = {k: s.field(k) for k in ("rho", "ux", "uy", "uz", "phi")}
+    status = s.check_status()
+    s.close()
+    del keep
+    return out, status
+
+
+def test_closure_identity_equals_plain_method():
+    plain, _ = _closure_run(None, None)
+    ident, st = _closure_run(0.0, 1.0)
+    assert st == 0
+    for k in plain:
+        assert np.array_equal(plain[k], ident[k]), k
+
+
+def test_closure_arrays_enter_the_step():
+    plain, _ = _closure_run(None, None)
+    visc, st = _closure_run(0.02, 1.0)
+    assert st == 0
+    assert not np.array_equal(plain["uz"], visc["uz"])
+    # more viscosity: the jet core slows less sharply but the field stays finite
+    assert np.all(np.isfinite(visc["uz"]))
+    surf, st2 = _closure_run(0.0, 2.0)
+    assert st2 == 0 and not np.array_equal(plain["ux"], surf["ux"])
