@@ -188,7 +188,7 @@ typedef struct ssmd_derived {
  * counterpart: the reference runs the plain method only.
  */
 typedef struct ssmd_closure {
-    const float *nut;         /* eddy viscosity (lattice units), >= 0          */
+    const float *nut;         /* eddy viscosity (lattice units), > -nu(phi)    */
     const float *sigma_scale; /* factor on sigma at the cell                   */
 } ssmd_closure;
 
@@ -426,11 +426,12 @@ int ssmd_check_status(const ssmd_params *p, uint32_t *status_out, ssmd_stream_t 
  * the subgrid stress tau_ij = <u_i u_j> - <u_i><u_j> (6 arrays: xx, yy, zz,
  * xy, xz, yz) and the mean fine |grad phi| (1 array).  ssmd_closure_targets
  * turns them into training targets on the coarse lattice: nu_t* =
- * clamp(-tau^d : S / (2 S:S + 1e-12), 0, nut_max) and sigma* = the ratio of
+ * clamp(-tau^d : S / (2 S:S + 1e-12), -nut_max, nut_max) and sigma* = the ratio of
  * the fine interface area density to the coarse one, 2 <|grad phi|> /
  * |grad phi_c|, clamped to [0.25, 4] (1 where |grad phi_c| < 1e-2), with
  * weights 1 and 4 phi (1 - phi) + 0.01.  ssmd_closure_apply evaluates the
- * network on features and writes nut = clamp(out0, 0, nut_max) and
+ * network on features and writes nut = clamp(out0, max(-nu(phi)/2, -nut_max),
+ * nut_max) (nu(phi) is feature 11) and
  * sigma_scale = clamp(out1, 0.25, 4); out is 2 * cells floats of scratch.
  */
 int ssmd_mlp_forward(const float *net, const float *features, int64_t n, float *out, ssmd_stream_t stream);

@@ -203,7 +203,7 @@ def targets(coarse, tau, area, per, nut_max):
             s = f32(0.5) * (d[a][b] + d[b][a])
             num += (t[a][b] - (tr if a == b else f32(0))) * s
             den += s * s
-    nut = np.clip(-num / (f32(2) * den + f32(1e-12)), 0, nut_max)
+    nut = np.clip(-num / (f32(2) * den + f32(1e-12)), -nut_max, nut_max)
     gx, gy, gz = _grad(phi, per)
     gm = np.sqrt(gx * gx + gy * gy + gz * gz)
     cs = np.where(gm >= f32(1e-2), np.clip(f32(2) * area / np.maximum(gm, f32(1e-30)), 0.25, 4.0), f32(1))

@@ -163,7 +163,8 @@ __global__ void targets_kernel(Grid g, const float *cf, const float *tau, const 
             num += (t[a][b] - (a == b ? tr : 0.f)) * s;
             den += s * s;
         }
-    const float nut = fminf(fmaxf(-num / (2.0f * den + 1e-12f), 0.0f), nut_max);
+    // signed: negative values (backscatter) are kept, the coarse run bounds them
+    const float nut = fminf(fmaxf(-num / (2.0f * den + 1e-12f), -nut_max), nut_max);
     float gx, gy, gz;
     grad3(g, phi, x, y, z, gx, gy, gz);
     const float gm = sqrtf(gx * gx + gy * gy + gz * gz);
@@ -176,10 +177,14 @@ __global__ void targets_kernel(Grid g, const float *cf, const float *tau, const 
     weights[2 * i + 1] = 4.0f * ph * (1.0f - ph) + 0.01f;
 }
 
-__global__ void apply_kernel(int64_t cells, const float *out, float nut_max, float *nut, float *cs) {
+// nu_t is bounded below by -nu(phi)/2 (feature 11), so the total viscosity
+// stays at least half the molecular one and the relaxation rate below 2.
+__global__ void apply_kernel(int64_t cells, const float *out, const float *feat, float nut_max, float *nut,
+                             float *cs) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= cells) return;
-    nut[i] = fminf(fmaxf(out[2 * i + 0], 0.0f), nut_max);
+    const float lo = fmaxf(-0.5f * feat[i * SSMD_MLP_IN + 11], -nut_max);
+    nut[i] = fminf(fmaxf(out[2 * i + 0], lo), nut_max);
     cs[i] = fminf(fmaxf(out[2 * i + 1], 0.25f), 4.0f);
 }
 
@@ -240,7 +245,7 @@ extern "C" int ssmd_closure_apply(const ssmd_params *coarse, const float *net, c
     if (!net || !features || !out || !nut || !sigma_scale) return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
     const int64_t cells = (int64_t)coarse->nx * coarse->ny * coarse->nz;
     if (int e = ssmd_mlp_forward(net, features, cells, out, stream)) return e;
-    apply_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(cells, out, nut_max, nut,
-                                                                                        sigma_scale);
+    apply_kernel<<<blocks_for(cells), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(cells, out, features,
+                                                                                        nut_max, nut, sigma_scale);
     return cuda_check(cudaGetLastError(), "closure apply launch");
 }

@@ -58,7 +58,7 @@ def test_filter_and_targets_shapes():
     assert coarse[0].shape == (4, 3, 2) and len(tau) == 6 and area.shape == (4, 3, 2)
     assert np.all(tau[0] >= -1e-9) and np.all(area >= 0)
     tg, w = co.targets(coarse, tau, area, (True, True, False), 0.05)
-    assert tg.shape == (24, 2) and np.all((tg[:, 0] >= 0) & (tg[:, 0] <= 0.05))
+    assert tg.shape == (24, 2) and np.all((tg[:, 0] >= -0.05) & (tg[:, 0] <= 0.05))
     assert np.all((tg[:, 1] >= 0.25) & (tg[:, 1] <= 4.0))
     feats = co.features(rho, *f, phi, (True, True, False), 0.01, 0.02)
     assert feats.shape == (phi.size, 12) and np.all(np.isfinite(feats))
