@@ -276,6 +276,71 @@ def run_sweep(steps: int = 40):
     return out
 
 
+def mlp_throughput(rows: int = 1 << 20, reps: int = 20):
+    """Device throughput of the closure network (tensor-core kernels)."""
+    import torch
+    from ssmdlbm_b200 import _lib
+    from ssmdlbm_b200.closure import Network
+    L = _lib.lib()
+    net = Network(0)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    feats = torch.randn(rows, _lib.MLP_IN, device="cuda", generator=g)
+    tg = torch.rand(rows, 2, device="cuda", generator=g)
+    out = torch.empty(rows, 2, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for name in ("forward", "grad"):
+        def once():
+            if name == "forward":
+                _lib.check(L.ssmd_mlp_forward(net.net.data_ptr(), feats.data_ptr(), rows, out.data_ptr(), st))
+            else:
+                _lib.check(L.ssmd_mlp_grad(net.net.data_ptr(), feats.data_ptr(), tg.data_ptr(), None, rows,
+                                           net.grad.data_ptr(), net.loss.data_ptr(), st))
+        for _ in range(3):
+            once()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            once()
+        e1.record()
+        e1.synchronize()
+        s_per = e0.elapsed_time(e1) / 1e3 / reps
+        flop = 2 * (12 * 64 + 64 * 64 + 64 * 2) * rows * (1 if name == "forward" else 3)
+        res[name] = {"rows_per_s": round(rows / s_per / 1e9, 3), "unit": "G rows/s", "ms": round(s_per * 1e3, 4),
+                     "tflops": round(flop / s_per / 1e12, 2)}
+    return res
+
+
+def run_closure(full: bool):
+    """Coarse-plus-closure run against the fine run it learns from (D3Q19 oil
+    jet, 2x coarsening).  Default: fine 128 x 128 x 512 for 4000 steps;
+    --closure-full: fine 256 x 256 x 1024 for 20000 steps (one seed)."""
+    from ssmdlbm_b200 import closure, configs
+    if full:
+        shape, steps, every, spin, train, diam = (256, 256, 1024), 20000, 1000, 10000, 4000, 32
+    else:
+        shape, steps, every, spin, train, diam = (128, 128, 512), 4000, 200, 2000, 2000, 16
+    fine = configs.oil_jet(*shape, 19, tau=0.55, sigma=1e-3, width=4.0, mobility=0.1, diam=diam, w_in=0.05,
+                           noise=0.01, seed=0)
+    r = closure.experiment(fine, steps=steps, sample_every=every, spinup=spin, train_steps=train, batch=65536,
+                           lr=1e-3, seed=0, update_every=10)
+    f, pl, cl = r["fine"], r["plain"], r["closure"]
+    return {
+        "workload": f"oil jet D3Q19+D3Q7 fine {shape[0]}x{shape[1]}x{shape[2]}, {steps} steps, nozzle {diam}, "
+                    f"tau 0.55, sigma 1e-3, M 0.1, w 0.05 + 1% noise; coarse 2x, {steps // 2} steps; "
+                    f"closure refreshed every 10 coarse steps",
+        "device_s": {"fine": round(f.device_s, 4), "coarse_plain": round(pl.device_s, 4),
+                     "coarse_closure": round(cl.device_s, 4), "training": round(r["train_device_s"], 4)},
+        "time_ratio_closure_vs_fine": round(cl.device_s / f.device_s, 4),
+        "errors_vs_fine": {k: {"plain": r["errors_plain"][k], "closure": r["errors_closure"][k]}
+                           for k in ("centreline_uz", "centreline_phi", "phi_volume", "droplets",
+                                     "droplet_volume")},
+        "heldout_loss": r["heldout_loss"], "samples": r["samples"], "mlp_status": r["mlp_status"],
+        "mlp": mlp_throughput(),
+    }
+
+
 def run_ours(a, world, rank, local):
     import torch
     from ssmdlbm_b200 import _lib
@@ -326,6 +391,7 @@ def run_ours(a, world, rank, local):
             torch.cuda.empty_cache()
 
     sweep = run_sweep() if not a.quick else None
+    closure_line = run_closure(a.closure_full) if (not a.quick and not a.no_closure) else None
 
     p.bulk_path, p.tile_z = sim_path, sim_tz
     e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
@@ -355,6 +421,7 @@ def run_ours(a, world, rank, local):
         "clocks": clocks,
         "variants": variants,
         "sweep": sweep,
+        "closure": closure_line,
         "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
     }
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -406,6 +473,9 @@ def main() -> int:
     ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--closure-full", action="store_true",
+                    help="closure leg at 256 x 256 x 1024, 20000 steps (minutes)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                     help="bulk kernel path: 0 auto, 1 gathers, 2 TMA phi boxes, 3 TMA population slabs")
     a = ap.parse_args()

@@ -75,6 +75,12 @@ typedef struct CUgraphExec_st *ssmd_graph_exec_t;
 
 /* ------------------------------------------------------------ step flags */
 #define SSMD_STEP_STORE_MACROS 1u /* write rho, ux, uy, uz, phi at every cell */
+#define SSMD_STEP_AVERAGE 2u      /* update the running means of ssmd_params.derived
+                                     in the step itself (no macroscopic store needed) */
+
+/* ssmd_derived_update: what to compute */
+#define SSMD_DERIVED_AVERAGES 1u  /* running means, t = number of updates so far + 1 */
+#define SSMD_DERIVED_VORTICITY 2u /* curl u and |curl u| from the stored u          */
 
 /* Closure network: 12 features -> 64 -> 64 -> 2, GELU.  A network is one FP32
  * device buffer of SSMD_MLP_NET_FLOATS: the SSMD_MLP_PARAMS trainable values
@@ -406,6 +412,18 @@ int ssmd_output_info(const char *dir, const char *id, const char *velocity_set, 
 /* Reads and clears the device status word (synchronises the stream):
  * bit 0 = a bulk cell produced a non-finite density. */
 int ssmd_check_status(const ssmd_params *p, uint32_t *status_out, ssmd_stream_t stream);
+
+/*
+ * Derived fields (reference DerivedFields::launch, src/derivedFields/
+ * DerivedFields.cuh:184-206, called once per step at src/main.cu:175): the
+ * non-null arrays of p->derived, from the macroscopic fields of the last
+ * step (run it with SSMD_STEP_STORE_MACROS).  Running means use t = (updates
+ * since ssmd_init) + 1, which is the reference's STEP + 1 when every step is
+ * averaged; a step with SSMD_STEP_AVERAGE performs the same update inside
+ * the step (bulk kernel for fluid cells, a ghost-layer pass after the
+ * boundaries) and counts as one update.  Device-side counter: graph-safe.
+ */
+int ssmd_derived_update(const ssmd_params *p, const LBMFields *fields, uint32_t what, ssmd_stream_t stream);
 
 /*
  * Learned closure (no reference counterpart).  The network runs on the

@@ -29,6 +29,9 @@ STORAGE_F16 = 1
 STORAGE_BF16 = 2
 
 STEP_STORE_MACROS = 1
+STEP_AVERAGE = 2
+DERIVED_AVERAGES = 1
+DERIVED_VORTICITY = 2
 
 PATH_AUTO = 0
 PATH_GATHER = 1
@@ -154,6 +157,7 @@ SIGNATURES = [
     ("ssmd_profile_enable", c_int32, [c_int32]),
     ("ssmd_profile_read", c_int32, [POINTER(c_float), c_int32, POINTER(c_int32)]),
     ("ssmd_profile_disable", c_int32, []),
+    ("ssmd_derived_update", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint32, c_void_p]),
     ("ssmd_mlp_forward", c_int32, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
     ("ssmd_mlp_grad", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,
                                 c_void_p]),

@@ -25,7 +25,7 @@ ROOT = os.path.dirname(HERE)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xptxas", "-v"]
-SOURCES = ["ssmd_api.cu", "kernels_q19.cu", "kernels_q27.cu", "reduce_static.cu", "stats.cu", "checkpoint.cu", "batch.cu", "mlp.cu", "closure.cu", "output.cpp"]
+SOURCES = ["ssmd_api.cu", "kernels_q19.cu", "kernels_q27.cu", "reduce_static.cu", "stats.cu", "checkpoint.cu", "batch.cu", "mlp.cu", "closure.cu", "derived.cu", "output.cpp"]
 
 
 def nvcc() -> str:

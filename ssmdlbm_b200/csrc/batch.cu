@@ -170,6 +170,8 @@ extern "C" int ssmd_batch_step(const ssmd_params *params, int32_t count, uint64_
                                void *table, ssmd_stream_t stream) {
     if (!params || count <= 0 || count > kMaxBatch || !table)
         return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument or bad batch size");
+    if (flags & ~SSMD_STEP_STORE_MACROS)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "batched steps take SSMD_STEP_STORE_MACROS only (0x%x)", flags);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     return dispatch(params[0].velocity_set, params[0].storage, [&](auto q, auto t) {
         return step<decltype(q)::value, decltype(t)>(params, count, step_index, flags, table, st);

@@ -497,6 +497,8 @@ struct Bulk {
             a.fld.pxz[c0] = m.pxz;
             a.fld.pyz[c0] = m.pyz;
         }
+        if (a.flags & SSMD_STEP_AVERAGE)
+            accumulate_averages(a.avg, c0, (float)(a.status->avg_t + 1u), phi, m.ux, m.uy, m.uz);
         if (!isfinite(m.rho)) atomicOr(&a.status->flags, 1u);
     }
 };

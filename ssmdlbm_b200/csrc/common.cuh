@@ -5,6 +5,7 @@
 #include <cuda_fp16.h>
 #include <cstdint>
 
+#include "../../include/ssmd.h"
 #include "lattice.cuh"
 
 namespace ssmd {
@@ -44,8 +45,35 @@ struct DeviceStatus {
     unsigned int pad0;
     unsigned long long step; // index of the step in progress (inlet noise)
     unsigned int work_next;  // persistent-kernel work counter
-    unsigned int pad1[11];
+    unsigned int avg_t;      // running-mean updates done (derived fields)
+    unsigned int pad1[10];
 };
+
+// Running means of the derived fields (null members are skipped).
+struct Averages {
+    float *phi, *ux, *uy, *uz;
+    float *uxux, *uyuy, *uzuz, *uxuy, *uxuz, *uyuz;
+};
+
+// avg <- avg + (v - avg) / t, every operation rounded on its own (no FMA),
+// the form of the reference's update (timeAverage.cuh:58-61).
+__device__ __forceinline__ float avg_update(float avg, float v, float t) {
+    return __fadd_rn(avg, __fdiv_rn(__fsub_rn(v, avg), t));
+}
+
+__device__ __forceinline__ void accumulate_averages(const Averages &A, uint64_t c, float t, float phi, float ux,
+                                                    float uy, float uz) {
+    if (A.phi) A.phi[c] = avg_update(A.phi[c], phi, t);
+    if (A.ux) A.ux[c] = avg_update(A.ux[c], ux, t);
+    if (A.uy) A.uy[c] = avg_update(A.uy[c], uy, t);
+    if (A.uz) A.uz[c] = avg_update(A.uz[c], uz, t);
+    if (A.uxux) A.uxux[c] = avg_update(A.uxux[c], __fmul_rn(ux, ux), t);
+    if (A.uyuy) A.uyuy[c] = avg_update(A.uyuy[c], __fmul_rn(uy, uy), t);
+    if (A.uzuz) A.uzuz[c] = avg_update(A.uzuz[c], __fmul_rn(uz, uz), t);
+    if (A.uxuy) A.uxuy[c] = avg_update(A.uxuy[c], __fmul_rn(ux, uy), t);
+    if (A.uxuz) A.uxuz[c] = avg_update(A.uxuz[c], __fmul_rn(ux, uz), t);
+    if (A.uyuz) A.uyuz[c] = avg_update(A.uyuz[c], __fmul_rn(uy, uz), t);
+}
 
 struct Geometry {
     uint32_t nx, ny, nz;
@@ -82,6 +110,7 @@ struct StepArgs {
     const TG *__restrict__ g_src;
     TG *__restrict__ g_dst;
     DeviceStatus *status;
+    Averages avg;         // derived running means (SSMD_STEP_AVERAGE)
     const float *clo_nut; // learned closure: eddy viscosity per cell (null: off)
     const float *clo_cs;  // learned closure: surface-tension factor per cell
     uint32_t flags;       // SSMD_STEP_*

@@ -111,7 +111,42 @@ static __global__ void set_status_kernel(DeviceStatus *s, unsigned long long ste
     s->flags = 0u;
     s->step = step;
     s->work_next = 0u;
+    s->avg_t = 0u;
 }
+
+inline Averages make_averages(const ssmd_params &p) {
+    Averages A{};
+    if (const ssmd_derived *d = p.derived) {
+        A.phi = d->avg_phi;
+        A.ux = d->avg_ux;
+        A.uy = d->avg_uy;
+        A.uz = d->avg_uz;
+        A.uxux = d->avg_uxux;
+        A.uyuy = d->avg_uyuy;
+        A.uzuz = d->avg_uzuz;
+        A.uxuy = d->avg_uxuy;
+        A.uxuz = d->avg_uxuz;
+        A.uyuz = d->avg_uyuz;
+    }
+    return A;
+}
+
+// Running means at cells the bulk kernel does not update (ghost layers), from
+// the macroscopic fields the boundary kernels wrote; t = avg_t + 1.
+static __global__ void averages_kernel(Geometry G, Fields F, Averages A, const DeviceStatus *status,
+                                       int ghost_only) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= G.cells) return;
+    if (ghost_only) {
+        const uint32_t c = (uint32_t)i;
+        const int x = c % G.nx, y = (c / G.nx) % G.ny, z = c / G.nxy;
+        if (x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi && z >= G.z_lo && z <= G.z_hi) return;
+    }
+    const float t = (float)(status->avg_t + 1u);
+    accumulate_averages(A, i, t, F.phi[i], F.ux[i], F.uy[i], F.uz[i]);
+}
+
+static __global__ void advance_avg_kernel(DeviceStatus *status) { status->avg_t += 1u; }
 
 // Dynamic shared memory of a bulk instantiation (TMA boxes or slabs).
 template <int Q, class T, int PATH>
@@ -175,6 +210,7 @@ template <class TF, class TG>
 inline void set_closure(StepArgs<TF, TG> &a, const ssmd_params &p) {
     a.clo_nut = p.closure ? p.closure->nut : nullptr;
     a.clo_cs = (p.closure && p.closure->nut) ? p.closure->sigma_scale : nullptr;
+    a.avg = make_averages(p);
 }
 
 template <int Q, class T>
@@ -237,6 +273,12 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     if (G.bcz == BC_JET) bc_outflow_z<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
     if (G.bcx == BC_COPY) bc_copy_x<Q, T, T><<<grid2(G.ny, G.nz), b2, 0, st>>>(a);
     if (G.bcy == BC_COPY) bc_copy_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+    if (flags & SSMD_STEP_AVERAGE) {
+        // the bulk kernel updated the fluid cells; the ghost layers follow, then t advances
+        const unsigned nb = (unsigned)((G.cells + 255) / 256);
+        averages_kernel<<<nb, 256, 0, st>>>(G, a.fld, a.avg, a.status, 1);
+        advance_avg_kernel<<<1, 1, 0, st>>>(a.status);
+    }
     return cuda_check(cudaGetLastError(), "boundary kernel launch");
 }
 

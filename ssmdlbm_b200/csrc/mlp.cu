@@ -3,11 +3,13 @@
 // Network: 12 features -> 64 -> 64 -> 2 outputs, GELU (erf form) after the
 // two hidden layers, features standardised by stored mean / inverse std,
 // outputs  p = scale * r + offset  with r the last layer's raw output.
-// One CTA of 128 threads handles 128 cells (thread i <-> cell row i):
+// A persistent CTA of 128 threads per SM loops over tiles of 128 cells
+// (thread i <-> cell row i of the tile), weights staged once per CTA:
 //   X [128 x 16] (bf16, K padded 12 -> 16)   z1 = X W1^T      (tcgen05, N = 64, K = 16)
 //   H1 = gelu(z1 + b1) [128 x 64] bf16        z2 = H1 W2^T     (4 MMAs of K = 16)
 //   H2 = gelu(z2 + b2) [128 x 64] bf16        r  = H2 W3^T     (N padded 2 -> 16)
-// Accumulators live in TMEM (z1: columns 0-63, z2: 64-127, r: 128-143); the
+// Accumulators live in TMEM (z1: columns 0-63, z2: 64-127, r: 128-143 when
+// training, 0-15 otherwise); the
 // epilogues read them back with tcgen05.ld, add the bias, apply GELU and
 // write the next layer's bf16 operand into shared memory.
 // Training (ssmd_mlp_grad) continues in the same CTA with the loss
@@ -15,8 +17,9 @@
 // and its backward pass: dH2 = dR W3 and dZ2 = dH2 gelu'(z2 + b2) on the CUDA
 // cores (N = 2 is too narrow for an MMA), dH1 = dZ2 W2 on the tensor cores
 // (TMEM columns 192-255), dZ1 = dH1 gelu'(z1 + b1); the weight and bias
-// gradients (sums over the CTA's 128 rows) on the CUDA cores, FP32, then
-// accumulated across CTAs with atomics.  Every wait on an MMA is bounded:
+// gradients (sums over a tile's 128 rows) on the CUDA cores in FP32,
+// carried in registers across the CTA's tiles and added across CTAs with
+// atomics once at the end.  Every wait on an MMA is bounded:
 // on timeout the CTA records bit 0 of the status word, frees its TMEM and
 // returns.
 #include <cuda_bf16.h>
@@ -39,8 +42,15 @@ constexpr int oMean = kParams, oInvStd = oMean + kIn, oScale = oInvStd + kIn, oO
 static_assert(kParams == SSMD_MLP_PARAMS, "parameter layout");
 static_assert(kNet == SSMD_MLP_NET_FLOATS, "network layout");
 
-constexpr uint32_t kTmemCols = 256;
-constexpr uint32_t cZ1 = 0, cZ2 = 64, cR = 128, cDH1 = 192;
+// TMEM columns: training keeps z1 and z2 for the backward pass (256 columns);
+// inference writes the last layer over z1, which is dead by then (128
+// columns), so four inference CTAs fit on an SM's 512 columns.
+template <bool TRAIN>
+constexpr uint32_t tmem_cols() { return TRAIN ? 256u : 128u; }
+template <bool TRAIN>
+constexpr uint32_t col_r() { return TRAIN ? 128u : 0u; }
+constexpr uint32_t cZ1 = 0, cZ2 = 64, cDH1 = 192;
+constexpr int kFwdCtasPerSm = 4;
 constexpr uint64_t kMmaWaitNs = 1000000000ull;
 constexpr int kLd = 65; // fp32 row stride of the dZ staging arrays (bank-conflict free)
 
@@ -119,7 +129,7 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bia
 }
 
 template <bool TRAIN>
-__global__ void __launch_bounds__(kThreadsMlp, 1)
+__global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
     mlp_kernel(const float *__restrict__ net, const float *__restrict__ feat, const float *__restrict__ target,
                const float *__restrict__ weight, int64_t n, float *__restrict__ out, float *__restrict__ grad,
                double *__restrict__ loss) {
@@ -138,7 +148,7 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
     volatile uint32_t *abort_flag = reinterpret_cast<volatile uint32_t *>(sm + L::abort);
 
     // ---- set-up: TMEM, barrier, weights, this CTA's features
-    if (warp == 0) umma::tmem_alloc(slot, kTmemCols);
+    if (warp == 0) umma::tmem_alloc(slot, tmem_cols<TRAIN>());
     if (tid == 0) {
         mbar_init(bar, 1);
         *abort_flag = 0u;
@@ -158,46 +168,57 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
     __syncthreads();
 
     const int r = tid;
-    const int64_t row = (int64_t)blockIdx.x * kRows + r;
-    const bool valid = row < n;
-    {
-        float x[kK1];
-#pragma unroll
-        for (int i = 0; i < kK1; ++i) {
-            float v = 0.f;
-            if (i < kIn && valid) v = (feat[row * kIn + i] - norm[i]) * norm[kIn + i];
-            x[i] = v;
-        }
-        st8(sm + sX, r, 0, kK1, x);
-        st8(sm + sX, r, 8, kK1, x + 8);
-    }
-    fence_proxy_async(); // generic-proxy smem writes -> visible to the tensor core
-    umma::fence_before_sync();
-    __syncthreads();
-    const uint32_t tmem = *slot;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     const uint32_t sbase = smem_addr(sm);
     uint32_t phase = 0;
     bool ok = true;
-
-    // ---- layer 1
-    if (tid == 0) {
-        umma::fence_after_sync();
-        umma::mma_bf16(tmem + cZ1, umma::smem_desc(sbase + sX, 128, 256), umma::smem_desc(sbase + sW1, 128, 256),
-                       umma::idesc_bf16(128, kH), false);
-        umma::commit(bar);
+    // weight-gradient partial sums of this CTA, carried across its tiles
+    float gw2[32], gw1[8], gw3 = 0.f, gb = 0.f, gb3 = 0.f;
+    if constexpr (TRAIN) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) gw2[i] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) gw1[i] = 0.f;
     }
-    ok = wait_mma(bar, phase, abort_flag);
-    phase ^= 1u;
-    if (ok) {
+    float lsum = 0.f;
+    const int64_t tiles = (n + kRows - 1) / kRows;
+    uint32_t tmem = 0, lane_base = 0;
+
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int64_t row = tile * kRows + r;
+        const bool valid = row < n;
+        {
+            float x[kK1];
+#pragma unroll
+            for (int i = 0; i < kK1; ++i) {
+                float v = 0.f;
+                if (i < kIn && valid) v = (feat[row * kIn + i] - norm[i]) * norm[kIn + i];
+                x[i] = v;
+            }
+            st8(sm + sX, r, 0, kK1, x);
+            st8(sm + sX, r, 8, kK1, x + 8);
+        }
+        fence_proxy_async(); // generic-proxy smem writes -> visible to the tensor core
+        umma::fence_before_sync();
+        __syncthreads(); // also: every TMEM read and MMA of the previous tile is complete
+        tmem = *slot;
+        lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+
+        // ---- layer 1
+        if (tid == 0) {
+            umma::fence_after_sync();
+            umma::mma_bf16(tmem + cZ1, umma::smem_desc(sbase + sX, 128, 256),
+                           umma::smem_desc(sbase + sW1, 128, 256), umma::idesc_bf16(128, kH), false);
+            umma::commit(bar);
+        }
+        ok = wait_mma(bar, phase, abort_flag);
+        phase ^= 1u;
+        if (!ok) break;
         hidden_epilogue(lane_base + cZ1, b1, sm + sH1, r);
         fence_proxy_async();
         umma::fence_before_sync();
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // ---- layer 2
-    if (ok) {
+        // ---- layer 2
         if (tid == 0) {
             umma::fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
@@ -208,62 +229,56 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
         }
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
-    }
-    if (ok) {
+        if (!ok) break;
         hidden_epilogue(lane_base + cZ2, b2, sm + sH2, r);
         fence_proxy_async();
         umma::fence_before_sync();
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // ---- layer 3 (N padded to 16; rows 2..15 of W3 are zero)
-    if (ok) {
+        // ---- layer 3 (N padded to 16; rows 2..15 of W3 are zero)
         if (tid == 0) {
             umma::fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
-                umma::mma_bf16(tmem + cR, umma::smem_desc(sbase + sH2 + 256 * ks, 128, 1024),
+                umma::mma_bf16(tmem + col_r<TRAIN>(), umma::smem_desc(sbase + sH2 + 256 * ks, 128, 1024),
                                umma::smem_desc(sbase + sW3 + 256 * ks, 128, 1024), umma::idesc_bf16(128, kN3),
                                ks > 0);
             umma::commit(bar);
         }
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
-    }
-    float rr[kOut] = {0.f, 0.f};
-    if (ok) {
-        float v[16];
-        umma::tmem_ld16(lane_base + cR, v);
-        rr[0] = v[0] + b3[0];
-        rr[1] = v[1] + b3[1];
+        if (!ok) break;
+        float rr[kOut];
+        {
+            float v[16];
+            umma::tmem_ld16(lane_base + col_r<TRAIN>(), v);
+            rr[0] = v[0] + b3[0];
+            rr[1] = v[1] + b3[1];
+        }
         if constexpr (!TRAIN) {
             if (valid) {
                 out[row * kOut + 0] = fmaf(norm[2 * kIn + 0], rr[0], norm[2 * kIn + 2]);
                 out[row * kOut + 1] = fmaf(norm[2 * kIn + 1], rr[1], norm[2 * kIn + 3]);
             }
-        }
-    }
-
-    if constexpr (TRAIN) {
-        float *dzf2 = reinterpret_cast<float *>(sm + sDZ2F);
-        float *dzf1 = reinterpret_cast<float *>(sm + sDZ1F);
-        float *dy = reinterpret_cast<float *>(sm + sDY);
-        // ---- loss and dL/dr
-        float lrow = 0.f, d0 = 0.f, d1 = 0.f;
-        if (ok && valid) {
-            const float inv_n = 1.0f / (float)n;
-            const float t0 = (target[row * kOut + 0] - norm[2 * kIn + 2]) / norm[2 * kIn + 0];
-            const float t1 = (target[row * kOut + 1] - norm[2 * kIn + 3]) / norm[2 * kIn + 1];
-            const float w0 = weight ? weight[row * kOut + 0] : 1.0f;
-            const float w1 = weight ? weight[row * kOut + 1] : 1.0f;
-            const float e0 = rr[0] - t0, e1 = rr[1] - t1;
-            lrow = w0 * e0 * e0 + w1 * e1 * e1;
-            d0 = 2.0f * w0 * e0 * inv_n;
-            d1 = 2.0f * w1 * e1 * inv_n;
-        }
-        dy[r * kOut + 0] = d0;
-        dy[r * kOut + 1] = d1;
-        // ---- dZ2 = (dR W3) * gelu'(z2 + b2)
-        if (ok) {
+        } else {
+            float *dzf2 = reinterpret_cast<float *>(sm + sDZ2F);
+            float *dzf1 = reinterpret_cast<float *>(sm + sDZ1F);
+            float *dy = reinterpret_cast<float *>(sm + sDY);
+            // ---- loss and dL/dr
+            float d0 = 0.f, d1 = 0.f;
+            if (valid) {
+                const float inv_n = 1.0f / (float)n;
+                const float t0 = (target[row * kOut + 0] - norm[2 * kIn + 2]) / norm[2 * kIn + 0];
+                const float t1 = (target[row * kOut + 1] - norm[2 * kIn + 3]) / norm[2 * kIn + 1];
+                const float w0 = weight ? weight[row * kOut + 0] : 1.0f;
+                const float w1 = weight ? weight[row * kOut + 1] : 1.0f;
+                const float e0 = rr[0] - t0, e1 = rr[1] - t1;
+                lsum += w0 * e0 * e0 + w1 * e1 * e1;
+                d0 = 2.0f * w0 * e0 * inv_n;
+                d1 = 2.0f * w1 * e1 * inv_n;
+            }
+            dy[r * kOut + 0] = d0;
+            dy[r * kOut + 1] = d1;
+            // ---- dZ2 = (dR W3) * gelu'(z2 + b2)
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 float v[16];
@@ -280,10 +295,8 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
             }
             fence_proxy_async();
             umma::fence_before_sync();
-        }
-        __syncthreads();
-        // ---- dH1 = dZ2 W2 (B = W2^T, K-major)
-        if (ok) {
+            __syncthreads();
+            // ---- dH1 = dZ2 W2 (B = W2^T, K-major)
             if (tid == 0) {
                 umma::fence_after_sync();
                 for (int ks = 0; ks < kH / 16; ++ks)
@@ -294,8 +307,7 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
             }
             ok = wait_mma(bar, phase, abort_flag);
             phase ^= 1u;
-        }
-        if (ok) {
+            if (!ok) break;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 float dh[16], z[16];
@@ -304,15 +316,10 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
 #pragma unroll
                 for (int i = 0; i < 16; ++i) dzf1[r * kLd + 16 * c + i] = dh[i] * gelu_grad(z[i] + b1[16 * c + i]);
             }
-        }
-        __syncthreads();
-        if (ok) {
-            // ---- weight and bias gradients: sums over the 128 rows
+            __syncthreads();
+            // ---- weight and bias gradients of this tile: sums over its 128 rows
             {   // dW2[o][i] = sum_r dZ2[r][o] H1[r][i]: thread -> (o, 32 i)
                 const int o = tid >> 1, i0 = (tid & 1) * 32;
-                float acc[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) acc[i] = 0.f;
                 for (int rr2 = 0; rr2 < kRows; ++rr2) {
                     const float d = dzf2[rr2 * kLd + o];
 #pragma unroll
@@ -323,19 +330,14 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
 #pragma unroll
                         for (int e = 0; e < 4; ++e) {
                             const float2 f2 = __bfloat1622float2(h[e]);
-                            acc[8 * ch + 2 * e] = fmaf(d, f2.x, acc[8 * ch + 2 * e]);
-                            acc[8 * ch + 2 * e + 1] = fmaf(d, f2.y, acc[8 * ch + 2 * e + 1]);
+                            gw2[8 * ch + 2 * e] = fmaf(d, f2.x, gw2[8 * ch + 2 * e]);
+                            gw2[8 * ch + 2 * e + 1] = fmaf(d, f2.y, gw2[8 * ch + 2 * e + 1]);
                         }
                     }
                 }
-#pragma unroll
-                for (int i = 0; i < 32; ++i) atomicAdd(&grad[oW2 + o * kH + i0 + i], acc[i]);
             }
             {   // dW1[o][i] = sum_r dZ1[r][o] X[r][i]: thread -> (o, 8 i)
                 const int o = tid >> 1, i0 = (tid & 1) * 8;
-                float acc[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) acc[i] = 0.f;
                 for (int rr2 = 0; rr2 < kRows; ++rr2) {
                     const float d = dzf1[rr2 * kLd + o];
                     const uint4 u = *reinterpret_cast<const uint4 *>(sm + sX + umma::kmajor_offset(rr2, i0, kK1));
@@ -343,31 +345,38 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const float2 f2 = __bfloat1622float2(h[e]);
-                        acc[2 * e] = fmaf(d, f2.x, acc[2 * e]);
-                        acc[2 * e + 1] = fmaf(d, f2.y, acc[2 * e + 1]);
+                        gw1[2 * e] = fmaf(d, f2.x, gw1[2 * e]);
+                        gw1[2 * e + 1] = fmaf(d, f2.y, gw1[2 * e + 1]);
                     }
                 }
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (i0 + i < kIn) atomicAdd(&grad[oW1 + o * kK1 + i0 + i], acc[i]);
             }
-            {   // dW3[k][j] = sum_r dR[r][k] H2[r][j]; db1, db2, db3
+            {   // dW3[k][j] = sum_r dR[r][k] H2[r][j]; db2 (k = 0 threads), db1 (k = 1); db3
                 const int k = tid >> 6, j = tid & 63;
-                float acc = 0.f, sb = 0.f;
                 for (int rr2 = 0; rr2 < kRows; ++rr2) {
-                    acc = fmaf(dy[rr2 * kOut + k], ldbf(sm + sH2, rr2, j, kH), acc);
-                    sb += k == 0 ? dzf2[rr2 * kLd + j] : dzf1[rr2 * kLd + j];
+                    gw3 = fmaf(dy[rr2 * kOut + k], ldbf(sm + sH2, rr2, j, kH), gw3);
+                    gb += k == 0 ? dzf2[rr2 * kLd + j] : dzf1[rr2 * kLd + j];
                 }
-                atomicAdd(&grad[oW3 + k * kH + j], acc);
-                atomicAdd(&grad[(k == 0 ? oB2 : oB1) + j], sb);
-                if (tid < kOut) {
-                    float s3 = 0.f;
-                    for (int rr2 = 0; rr2 < kRows; ++rr2) s3 += dy[rr2 * kOut + tid];
-                    atomicAdd(&grad[oB3 + tid], s3);
-                }
+                if (tid < kOut)
+                    for (int rr2 = 0; rr2 < kRows; ++rr2) gb3 += dy[rr2 * kOut + tid];
             }
-            // ---- loss
-            float l = lrow;
+            __syncthreads(); // the next tile overwrites X, H1, H2 and the dZ staging
+        }
+    }
+
+    if constexpr (TRAIN) {
+        if (ok) {
+            const int o = tid >> 1;
+            const int i0 = (tid & 1) * 32, i1 = (tid & 1) * 8;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) atomicAdd(&grad[oW2 + o * kH + i0 + i], gw2[i]);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (i1 + i < kIn) atomicAdd(&grad[oW1 + o * kK1 + i1 + i], gw1[i]);
+            const int k = tid >> 6, j = tid & 63;
+            atomicAdd(&grad[oW3 + k * kH + j], gw3);
+            atomicAdd(&grad[(k == 0 ? oB2 : oB1) + j], gb);
+            if (tid < kOut) atomicAdd(&grad[oB3 + tid], gb3);
+            float l = lsum;
             for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
             if ((tid & 31) == 0) atomicAdd(loss, (double)l / (double)n);
         }
@@ -377,7 +386,7 @@ __global__ void __launch_bounds__(kThreadsMlp, 1)
     umma::fence_before_sync();
     __syncthreads();
     if (!ok && tid == 0) atomicOr(&g_mlp_status, 1u);
-    if (warp == 0) umma::tmem_dealloc(tmem, kTmemCols);
+    if (warp == 0) umma::tmem_dealloc(*slot, tmem_cols<TRAIN>());
 }
 
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
@@ -396,9 +405,11 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
 template <bool TRAIN>
 int launch(const float *net, const float *feat, const float *target, const float *weight, int64_t n, float *out,
            float *grad, double *loss, cudaStream_t st) {
-    // at least 120 KB: one CTA per SM, so every resident CTA can hold its 256
-    // TMEM columns (an SM has 512) without waiting in tcgen05.alloc
-    const size_t smem = Layout<TRAIN>::bytes > (size_t)120 * 1024 ? Layout<TRAIN>::bytes : (size_t)120 * 1024;
+    // shared memory sized so that at most 512 / tmem_cols CTAs share an SM:
+    // every resident CTA then holds its TMEM columns without waiting in
+    // tcgen05.alloc (training: 1 per SM, inference: 4 per SM)
+    const size_t floor_bytes = TRAIN ? (size_t)120 * 1024 : (size_t)52 * 1024;
+    const size_t smem = Layout<TRAIN>::bytes > floor_bytes ? Layout<TRAIN>::bytes : floor_bytes;
     static bool attr_set = false;
     if (!attr_set) {
         if (int e = cuda_check(cudaFuncSetAttribute(mlp_kernel<TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -407,7 +418,16 @@ int launch(const float *net, const float *feat, const float *target, const float
             return e;
         attr_set = true;
     }
-    const unsigned blocks = (unsigned)((n + kRows - 1) / kRows);
+    // persistent: one CTA per SM, each loops over 128-row tiles
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const int64_t tiles = (n + kRows - 1) / kRows;
+    const int64_t slots = (int64_t)sms * (TRAIN ? 1 : kFwdCtasPerSm);
+    const unsigned blocks = (unsigned)(tiles < slots ? tiles : slots);
     mlp_kernel<TRAIN><<<blocks, kThreadsMlp, smem, st>>>(net, feat, target, weight, n, out, grad, loss);
     return cuda_check(cudaGetLastError(), "mlp launch");
 }

@@ -253,6 +253,10 @@ int ssmd_step(LBMFields *fields, const ssmd_params *p, uint64_t step, uint32_t f
               ssmd_stream_t stream) {
     if (int e = ssmd_validate(p)) return e;
     if (int e = check_fields(*p, fields)) return e;
+    if (flags & ~(SSMD_STEP_STORE_MACROS | SSMD_STEP_AVERAGE))
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "unknown step flags 0x%x", flags);
+    if ((flags & SSMD_STEP_AVERAGE) && !p->derived)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "SSMD_STEP_AVERAGE needs params.derived");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     switch (p->velocity_set * 4 + p->storage) {
     case 19 * 4 + SSMD_STORAGE_F32: return launch_step<19, float>(*p, *fields, step, flags, st);

@@ -90,14 +90,40 @@ class Simulation:
         check(lib().ssmd_init_from_macros(ctypes.byref(self.p), ctypes.byref(self.fields), self.stream))
         self.steps_done = 0
 
-    def step(self, n: int = 1, store_macros: bool = False) -> None:
+    def step(self, n: int = 1, store_macros: bool = False, average: bool = False) -> None:
+        """n steps; store_macros: the last one writes the macroscopic fields;
+        average: every step updates the running means (enable_derived first)."""
         L = lib()
         for i in range(n):
             last = i == n - 1
             flags = _lib.STEP_STORE_MACROS if (store_macros and last) else 0
+            if average:
+                flags |= _lib.STEP_AVERAGE
             check(L.ssmd_step(ctypes.byref(self.fields), ctypes.byref(self.p), self.steps_done, flags,
                               self.stream))
             self.steps_done += 1
+
+    # ------------------------------------------------------- derived fields
+    DERIVED = ("avg_phi", "avg_ux", "avg_uy", "avg_uz", "avg_uxux", "avg_uyuy", "avg_uzuz", "avg_uxuy",
+               "avg_uxuz", "avg_uyuz", "vort_x", "vort_y", "vort_z", "vort_mag")
+
+    def enable_derived(self, names=None) -> None:
+        """Allocate (zeroed) derived-field arrays; names defaults to all of them."""
+        names = self.DERIVED if names is None else tuple(names)
+        self._derived = _lib.Derived()
+        for k in names:
+            if k not in self.DERIVED:
+                raise KeyError(k)
+            self.t[k] = torch.zeros(self.cells, dtype=torch.float32, device=self.device)
+            setattr(self._derived, k, self.t[k].data_ptr())
+        self.p.derived = ctypes.addressof(self._derived)
+        for ex in self._graphs.values():
+            check(lib().ssmd_graph_destroy(ex))
+        self._graphs.clear()
+
+    def derived_update(self, what: int = _lib.DERIVED_AVERAGES | _lib.DERIVED_VORTICITY) -> None:
+        """The reference's per-step derived-field launch, from the stored macroscopic fields."""
+        check(lib().ssmd_derived_update(ctypes.byref(self.p), ctypes.byref(self.fields), what, self.stream))
 
     def graph(self, steps: int = 2, flags: int = 0) -> int:
         """Instantiate (once) a CUDA graph of `steps` steps starting at the current parity."""
