@@ -384,6 +384,16 @@ int ssmd_checkpoint_load(const ssmd_params *p, LBMFields *fields, const char *pa
  *   the HOST array out (unordered) and the number found to *n_out
  *   (SSMD_ERR_INVALID_ARGUMENT when more than max_droplets exist).  Needs
  *   ssmd_droplets_scratch_bytes() bytes of device scratch.  Synchronises.  */
+/*
+ * Phase-field budget of the step that produced `steps_done`: the FP64 sums of
+ * the D3Q7 populations that stream from ghost cells into the fluid region
+ * (inflow) and from the fluid region into ghost cells (outflow), so that
+ * sum phi after the next gather = sum phi before + inflow - outflow
+ * (ssmd_stats.phi_sum_next before and after).  Synchronous; uses the
+ * workspace, like ssmd_reduce.  No reference counterpart.
+ */
+int ssmd_phase_flux(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done, double *inflow,
+                    double *outflow, ssmd_stream_t stream);
 int ssmd_centreline(const ssmd_params *p, const LBMFields *fields, double *uz_out, double *phi_out,
                     ssmd_stream_t stream);
 size_t ssmd_droplets_scratch_bytes(const ssmd_params *p, int32_t max_droplets);

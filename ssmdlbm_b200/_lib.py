@@ -157,6 +157,8 @@ SIGNATURES = [
     ("ssmd_profile_enable", c_int32, [c_int32]),
     ("ssmd_profile_read", c_int32, [POINTER(c_float), c_int32, POINTER(c_int32)]),
     ("ssmd_profile_disable", c_int32, []),
+    ("ssmd_phase_flux", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint64, POINTER(c_double),
+                                  POINTER(c_double), c_void_p]),
     ("ssmd_derived_update", c_int32, [POINTER(Params), POINTER(LBMFields), c_uint32, c_void_p]),
     ("ssmd_mlp_forward", c_int32, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
     ("ssmd_mlp_grad", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,

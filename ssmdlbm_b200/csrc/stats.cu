@@ -149,6 +149,48 @@ __global__ void ccl_collect(Geometry G, DropScratch S) {
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Phase-field populations that cross the boundary of the fluid region in the
+// step just taken.  In the pull layout fluid cell x gathers direction q from
+// slot q of x - c_q, so phi enters from ghost slots (q, x - c_q) and leaves
+// through the fluid slots (q, x) whose x + c_q is a ghost cell.  FP64 sums;
+// with the collision conserving phi per cell this closes the budget
+// sum phi^{n+1} = sum phi^n + inflow - outflow.
+template <class TG>
+__global__ void phase_flux_kernel(Geometry G, const TG *g, double *acc) {
+    __shared__ double s_in[256], s_out[256];
+    double in = 0.0, out = 0.0;
+    const bool per[3] = {G.bcx == BC_PERIODIC, G.bcy == BC_PERIODIC, G.bcz == BC_PERIODIC};
+    const int n[3] = {(int)G.nx, (int)G.ny, (int)G.nz};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < G.cells;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)i;
+        const int p[3] = {(int)(c % G.nx), (int)((c / G.nx) % G.ny), (int)(c / G.nxy)};
+        if (!fluid_cell(G, p[0], p[1], p[2])) continue;
+        for (int q = 1; q < 7; ++q) {
+            const int axis = (q - 1) >> 1, sgn = (q & 1) ? 1 : -1; // 1:+x 2:-x 3:+y 4:-y 5:+z 6:-z
+            int a[3] = {p[0], p[1], p[2]}, b[3] = {p[0], p[1], p[2]};
+            a[axis] = axis_nb(p[axis] - sgn, n[axis], per[axis]); // source of direction q
+            b[axis] = axis_nb(p[axis] + sgn, n[axis], per[axis]); // where this cell's q goes
+            if (!fluid_cell(G, a[0], a[1], a[2])) in += (double)Store<TG>::ld(g + slot(G, q, cell_index(G, a[0], a[1], a[2])));
+            if (!fluid_cell(G, b[0], b[1], b[2])) out += (double)Store<TG>::ld(g + slot(G, q, c));
+        }
+    }
+    s_in[threadIdx.x] = in;
+    s_out[threadIdx.x] = out;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            s_in[threadIdx.x] += s_in[threadIdx.x + w];
+            s_out[threadIdx.x] += s_out[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[0], s_in[0]);
+        atomicAdd(&acc[1], s_out[0]);
+    }
+}
+
 } // namespace
 
 extern "C" int ssmd_centreline(const ssmd_params *p, const LBMFields *fields, double *uz_out, double *phi_out,
@@ -217,4 +259,32 @@ extern "C" int ssmd_droplets(const ssmd_params *p, const LBMFields *fields, floa
     return found > (uint32_t)max_droplets
                ? fail(SSMD_ERR_INVALID_ARGUMENT, "%u droplets found, only %d returned", found, max_droplets)
                : SSMD_OK;
+}
+
+extern "C" int ssmd_phase_flux(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done, double *inflow,
+                               double *outflow, ssmd_stream_t stream) {
+    if (int e = ssmd_validate(p)) return e;
+    if (int e = check_fields(*p, fields)) return e;
+    if (!inflow || !outflow) return fail(SSMD_ERR_INVALID_ARGUMENT, "null output");
+    const Geometry G = make_geometry(*p);
+    const void *g = (steps_done & 1ull) == 0ull ? fields->g : p->g_alt;
+    double *acc = reinterpret_cast<double *>(static_cast<char *>(p->workspace) + kPartialOff);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (int e = cuda_check(cudaMemsetAsync(acc, 0, 2 * sizeof(double), st), "flux clear")) return e;
+    uint64_t nb64 = (G.cells + 255) / 256;
+    const unsigned nb = (unsigned)(nb64 < 4096 ? nb64 : 4096);
+    switch (p->storage) {
+    case SSMD_STORAGE_F32: phase_flux_kernel<float><<<nb, 256, 0, st>>>(G, static_cast<const float *>(g), acc); break;
+    case SSMD_STORAGE_F16: phase_flux_kernel<__half><<<nb, 256, 0, st>>>(G, static_cast<const __half *>(g), acc); break;
+    default:
+        phase_flux_kernel<__nv_bfloat16><<<nb, 256, 0, st>>>(G, static_cast<const __nv_bfloat16 *>(g), acc);
+        break;
+    }
+    if (int e = cuda_check(cudaGetLastError(), "flux launch")) return e;
+    double h[2] = {0.0, 0.0};
+    if (int e = cuda_check(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, st), "flux copy")) return e;
+    if (int e = cuda_check(cudaStreamSynchronize(st), "flux sync")) return e;
+    *inflow = h[0];
+    *outflow = h[1];
+    return SSMD_OK;
 }

@@ -165,6 +165,13 @@ class Simulation:
                                          ctypes.byref(n), self.stream))
         self.steps_done = int(n.value)
 
+    def phase_flux(self) -> tuple:
+        """(inflow, outflow) of phi in the last step, FP64."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(lib().ssmd_phase_flux(ctypes.byref(self.p), ctypes.byref(self.fields), self.steps_done,
+                                    ctypes.byref(a), ctypes.byref(b), self.stream))
+        return a.value, b.value
+
     def centreline(self):
         """Mean u_z and phi along the oil-nozzle axis, per z (FP64 numpy arrays).
         Needs the macroscopic fields of a step with store_macros."""
