@@ -74,6 +74,7 @@ int prepare(const ssmd_params *params, const LBMFields *fields, int32_t count, v
             a.f_dst = static_cast<T *>(even ? p.f_alt : fl.f);
             a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
             a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
+            set_bases(a, Q);
             a.status = status_of(p);
             set_closure(a, p);
             a.flags = 0;

@@ -93,15 +93,13 @@ struct Bulk {
         const uint32_t yp = c + (y == (int)G.ny - 1 ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx);
         const uint32_t zm = c + (z == 0 ? (uint32_t)(G.cells - G.nxy) : (uint32_t)-(int)G.nxy);
         const uint32_t zp = c + (z == (int)G.nz - 1 ? (uint32_t)-(int64_t)(G.cells - G.nxy) : G.nxy);
-        const TG *g = a.g_src;
-        const uint64_t N = G.cells;
-        float s = Store<TG>::ld(g + c);
-        s += Store<TG>::ld(g + 1 * N + xm);
-        s += Store<TG>::ld(g + 2 * N + xp);
-        s += Store<TG>::ld(g + 3 * N + ym);
-        s += Store<TG>::ld(g + 4 * N + yp);
-        s += Store<TG>::ld(g + 5 * N + zm);
-        s += Store<TG>::ld(g + 6 * N + zp);
+        float s = Store<TG>::ld(a.gq_src[0] + c);
+        s += Store<TG>::ld(a.gq_src[1] + xm);
+        s += Store<TG>::ld(a.gq_src[2] + xp);
+        s += Store<TG>::ld(a.gq_src[3] + ym);
+        s += Store<TG>::ld(a.gq_src[4] + yp);
+        s += Store<TG>::ld(a.gq_src[5] + zm);
+        s += Store<TG>::ld(a.gq_src[6] + zp);
         return s;
     }
 
@@ -420,8 +418,8 @@ struct Bulk {
         float gin[7];
         const bool bgk = a.phys.omega_g != 1.0f;
         if (fs == nullptr) {
-            unroll<0, Q>([&](auto q) { f[q] = Store<TF>::ld(a.f_src + (uint64_t)q * N + src(q)); });
-            if (bgk) unroll<0, 7>([&](auto q) { gin[q] = Store<TG>::ld(a.g_src + (uint64_t)q * N + src(q)); });
+            unroll<0, Q>([&](auto q) { f[q] = Store<TF>::ld(a.fq_src[q] + src(q)); });
+            if (bgk) unroll<0, 7>([&](auto q) { gin[q] = Store<TG>::ld(a.gq_src[q] + src(q)); });
         } else {
             // slab path: immediate shared-memory offsets; lanes whose source wraps an
             // exact-periodic x or y axis (outside the slab) reload those directions
@@ -440,13 +438,13 @@ struct Bulk {
                 unroll<0, Q>([&](auto q) {
                     constexpr int cx = cx27(q), cy = cy27(q);
                     const bool w = (cx > 0 && wx0) || (cx < 0 && wx1) || (cy > 0 && wy0) || (cy < 0 && wy1);
-                    if (w) f[q] = Store<TF>::ld(a.f_src + (uint64_t)q * N + src(q));
+                    if (w) f[q] = Store<TF>::ld(a.fq_src[q] + src(q));
                 });
                 if (bgk)
                     unroll<0, 7>([&](auto q) {
                         constexpr int cx = cx27(q), cy = cy27(q);
                         const bool w = (cx > 0 && wx0) || (cx < 0 && wx1) || (cy > 0 && wy0) || (cy < 0 && wy1);
-                        if (w) gin[q] = Store<TG>::ld(a.g_src + (uint64_t)q * N + src(q));
+                        if (w) gin[q] = Store<TG>::ld(a.gq_src[q] + src(q));
                     });
             }
         }
@@ -458,7 +456,7 @@ struct Bulk {
         const float omega = __frcp_rn(0.5f + 3.0f * nu); // = 1 / (...), correctly rounded
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
-        unroll<0, Q>([&](auto q) { Store<TF>::st(a.f_dst + (uint64_t)q * N + c0, fo[q]); });
+        unroll<0, Q>([&](auto q) { Store<TF>::st(a.fq_dst[q] + c0, fo[q]); });
 
         // ---- conservative Allen-Cahn update, D3Q7 (lbm.cu:256-269; D3Q7.cuh:124-148)
         const float sharp = P.gamma * phi * (1.0f - phi);
@@ -478,7 +476,7 @@ struct Bulk {
             // reduces to the reference's g = g_eq + h.
             unroll<0, 7>([&](auto q) { go[q] = gin[q] + P.omega_g * (go[q] - gin[q]); });
         }
-        unroll<0, 7>([&](auto q) { Store<TG>::st(a.g_dst + (uint64_t)q * N + c0, go[q]); });
+        unroll<0, 7>([&](auto q) { Store<TG>::st(a.gq_dst[q] + c0, go[q]); });
 
         // ---- macroscopic fields needed by the boundaries (or all, on save steps)
         const bool bplane = (G.bcx == BC_COPY && (x == 1 || x == (int)G.nx - 2)) ||

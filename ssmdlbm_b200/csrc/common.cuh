@@ -109,6 +109,13 @@ struct StepArgs {
     TF *__restrict__ f_dst;
     const TG *__restrict__ g_src;
     TG *__restrict__ g_dst;
+    // per-direction bases f_src + q N, ... (set_bases): the bulk kernel reads
+    // them from the parameter space, so every population access is a 32-bit
+    // cell index scaled onto a base the kernel does not compute
+    const TF *fq_src[27];
+    TF *fq_dst[27];
+    const TG *gq_src[7];
+    TG *gq_dst[7];
     DeviceStatus *status;
     Averages avg;         // derived running means (SSMD_STEP_AVERAGE)
     const float *clo_nut; // learned closure: eddy viscosity per cell (null: off)
@@ -118,6 +125,18 @@ struct StepArgs {
     int zchunk, nzchunks;
     int halo_mod;         // 1: a tile halo may wrap a periodic axis more than once
 };
+
+template <class TF, class TG>
+inline void set_bases(StepArgs<TF, TG> &a, int Q) {
+    for (int q = 0; q < 27; ++q) {
+        a.fq_src[q] = q < Q ? a.f_src + (uint64_t)q * a.geo.cells : nullptr;
+        a.fq_dst[q] = q < Q ? a.f_dst + (uint64_t)q * a.geo.cells : nullptr;
+    }
+    for (int q = 0; q < 7; ++q) {
+        a.gq_src[q] = a.g_src + (uint64_t)q * a.geo.cells;
+        a.gq_dst[q] = a.g_dst + (uint64_t)q * a.geo.cells;
+    }
+}
 
 // ------------------------------------------------------------- indexing
 __host__ __device__ __forceinline__ uint32_t cell_index(const Geometry &g, uint32_t x, uint32_t y,

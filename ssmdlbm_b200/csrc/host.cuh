@@ -225,6 +225,7 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     a.f_dst = static_cast<T *>(even ? p.f_alt : fl.f);
     a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
     a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
+    set_bases(a, Q);
     a.status = status_of(p);
     set_closure(a, p);
     a.flags = flags;
