@@ -14,9 +14,10 @@
 // both buffers.
 //
 // Work item: a 32 x 8 column of cells marching over `zchunk` z planes.  phi is
-// rebuilt from g on the fly (never re-read from DRAM) into a 5-plane ring with
-// a 2-cell halo; interface normals and |grad phi| live in a 2-plane ring with a
-// 1-cell halo; the curvature stencil is split into per-plane partial sums
+// rebuilt from g on the fly (never re-read from DRAM) into a 6-plane ring with
+// a 2-cell halo; interface normals and |grad phi| live in a 3-plane ring with a
+// 1-cell halo, both filled ahead of the plane being updated so that one barrier
+// per plane suffices; the curvature stencil is split into per-plane partial sums
 // that each thread carries along its own column in registers; the
 // populations of the cell are gathered straight from DRAM (pull) and written
 // back to the cell's own slots (aligned, coalesced).
@@ -66,14 +67,14 @@ struct Slab {
 };
 
 struct BulkSmem {
-    float phiR[5][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
-    float phiZ[5][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
-    float nrm[2][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field, slot = plane & 1
+    float phiR[6][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
+    float phiZ[6][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
+    float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
 };
 
 // Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
-__device__ __forceinline__ int ring5(int p) { return (int)((unsigned)(p + 10) % 5u); }
-__device__ __forceinline__ int ring2(int p) { return p & 1; }
+__device__ __forceinline__ int ringP(int p) { return (int)((unsigned)(p + 12) % 6u); } // phi: 6 planes
+__device__ __forceinline__ int ringN(int p) { return (int)((unsigned)(p + 3) % 3u); }  // normals: 3 planes
 
 template <int Q, class TF, class TG>
 struct Bulk {
@@ -115,28 +116,58 @@ struct Bulk {
         return axis_nb(c, n, periodic);
     }
 
+    // The phi ring of a plane (36 x 12 cells: the tile and a 2-cell border)
+    // is filled one element per thread for the thread's own column and one
+    // more for tid < kPhiBorder, which covers the border: rows 0-1 and 10-11,
+    // then columns 0, 1, 34, 35 of rows 2-9.
+    static constexpr int kPhiBorder = kHX * kHY - kThreads; // 176
+    static __device__ __forceinline__ void phi_border_pos(int tid, int &hx, int &hy) {
+        if (tid < 2 * kHX) {
+            hy = tid / kHX;
+            hx = tid - hy * kHX;
+        } else if (tid < 4 * kHX) {
+            const int k = tid - 2 * kHX, r = k / kHX;
+            hy = kHY - 2 + r;
+            hx = k - r * kHX;
+        } else {
+            const int k = tid - 4 * kHX, c = k & 3;
+            hy = 2 + (k >> 2);
+            hx = c < 2 ? c : kHX - 4 + c;
+        }
+    }
+
+    // phi of ring element (hx, hy) = lattice cell (rx, ry) before wrapping, plane gz.
+    static __device__ __forceinline__ void phi_elem(const A &a, BulkSmem &S, int s, int hx, int hy, int rx, int ry,
+                                                    int gz, bool zfluid) {
+        const Geometry &G = a.geo;
+        const int gx = halo_axis(a, rx, G.nx, G.bcx == BC_PERIODIC);
+        const int gy = halo_axis(a, ry, G.ny, G.bcy == BC_PERIODIC);
+        float raw = 0.f, zer = 0.f;
+        if (gx >= 0 && gy >= 0 && gz >= 0) {
+            const uint32_t c = cell_index(G, gx, gy, gz);
+            if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
+                raw = phi_from_g(a, gx, gy, gz, c);
+                zer = raw;
+            } else {
+                raw = a.fld.phi[c];
+            }
+        }
+        S.phiR[s][hy][hx] = raw;
+        S.phiZ[s][hy][hx] = zer;
+    }
+
     // Fill ring slot of plane pz with phi over the tile + 2-cell halo.
     static __device__ void fill_phi(const A &a, BulkSmem &S, int x0, int y0, int pz, int tid) {
         const Geometry &G = a.geo;
         const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
-        const int s = ring5(pz);
+        const int s = ringP(pz);
         const bool zfluid = gz >= G.z_lo && gz <= G.z_hi;
-        for (int i = tid; i < kHX * kHY; i += kThreads) {
-            const int hx = i % kHX, hy = i / kHX;
-            const int gx = halo_axis(a, x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
-            const int gy = halo_axis(a, y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
-            float raw = 0.f, zer = 0.f;
-            if (gx >= 0 && gy >= 0 && gz >= 0) {
-                const uint32_t c = cell_index(G, gx, gy, gz);
-                if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
-                    raw = phi_from_g(a, gx, gy, gz, c);
-                    zer = raw;
-                } else {
-                    raw = a.fld.phi[c];
-                }
-            }
-            S.phiR[s][hy][hx] = raw;
-            S.phiZ[s][hy][hx] = zer;
+        const int tx = tid % kTX, ty = tid / kTX;
+        phi_elem(a, S, s, tx + 2, ty + 2, x0 + tx, y0 + ty, gz, zfluid);
+        if (tid < kPhiBorder) {
+            int hx, hy;
+            phi_border_pos(tid, hx, hy);
+            phi_elem(a, S, s, hx, hy, x0 - 2 + hx, y0 - 2 + hy, gz, zfluid);
         }
     }
 
@@ -153,7 +184,7 @@ struct Bulk {
         const Geometry &G = a.geo;
         const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC;
         const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
-        const int s = ring5(pz);
+        const int s = ringP(pz);
         const bool zfluid = gz >= G.z_lo && gz <= G.z_hi;
         for (int i = tid; i < kHX * kHY; i += kThreads) {
             const int hx = i % kHX, hy = i / kHX;
@@ -203,26 +234,29 @@ struct Bulk {
     }
 
     // One work item on the gather path: the 32 x 8 column at (x0, y0) over
-    // planes [zs, ze).  Ends with a block-wide barrier.
+    // planes [zs, ze).  One barrier per plane: iteration z updates plane z
+    // and fills the normals of plane z + 2 and phi of plane z + 4, which
+    // later iterations read; the ring slots they overwrite (z - 1, z - 2)
+    // were last read before the previous barrier, so the gathers of the
+    // cell update and the stencil arithmetic of the fills interleave freely.
+    // Ends with a block-wide barrier.
     static __device__ void run_gather(const A &a, BulkSmem &S, int x0, int y0, int zs, int ze, int tx, int ty,
                                       int tid) {
         const Geometry &G = a.geo;
         const int x = x0 + tx, y = y0 + ty;
         const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
-        for (int p = zs - 2; p <= zs + 2; ++p) fill_phi(a, S, x0, y0, p, tid);
+        for (int p = zs - 2; p <= zs + 3; ++p) fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
-        fill_nrm(S, zs - 1, tid);
-        fill_nrm(S, zs, tid);
+        for (int p = zs - 1; p <= zs + 1; ++p) fill_nrm(S, p, tid);
         __syncthreads();
         Curv cv;
         cv.start(S, zs, tx, ty);
         __syncthreads();
         for (int z = zs; z < ze; ++z) {
-            fill_nrm(S, z + 1, tid);
-            __syncthreads();
             const float div = cv.advance(S, z, tx, ty);
             if (active) cell(a, S, x, y, z, tx, ty, div);
-            if (z + 1 < ze) fill_phi(a, S, x0, y0, z + 3, tid);
+            if (z + 2 <= ze) fill_nrm(S, z + 2, tid);
+            if (z + 4 <= ze + 1) fill_phi(a, S, x0, y0, z + 4, tid);
             __syncthreads();
         }
     }
@@ -274,20 +308,44 @@ struct Bulk {
         gz = 3.0f * sz;
     }
 
+    // The normal ring (34 x 10) is filled like the phi ring: the thread's own
+    // column, and for tid < kNrmBorder one element of the 1-cell border (rows 0
+    // and 9, then columns 0 and 33 of rows 1-8).
+    static constexpr int kNrmBorder = kNX * kNY - kThreads; // 84
+    static __device__ __forceinline__ void nrm_border_pos(int tid, int &nxh, int &nyh) {
+        if (tid < kNX) {
+            nxh = tid;
+            nyh = 0;
+        } else if (tid < 2 * kNX) {
+            nxh = tid - kNX;
+            nyh = kNY - 1;
+        } else {
+            const int k = tid - 2 * kNX;
+            nyh = 1 + (k >> 1);
+            nxh = (k & 1) ? kNX - 1 : 0;
+        }
+    }
+
+    static __device__ __forceinline__ void nrm_elem(BulkSmem &S, int s, int sm, int s0, int sp, int nxh, int nyh) {
+        float gx, gy, gz;
+        grad(S.phiZ, nxh + 1, nyh + 1, sm, s0, sp, gx, gy, gz);
+        const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
+        const float inv = __frcp_rn(ind + 1e-9f); // = 1 / (ind + 1e-9), correctly rounded
+        S.nrm[s][0][nyh][nxh] = gx * inv;
+        S.nrm[s][1][nyh][nxh] = gy * inv;
+        S.nrm[s][2][nyh][nxh] = gz * inv;
+        S.nrm[s][3][nyh][nxh] = ind;
+    }
+
     // Normals and |grad phi| of plane pz over the tile + 1-cell halo.
     static __device__ void fill_nrm(BulkSmem &S, int pz, int tid) {
-        const int s = ring2(pz);
-        const int sm = ring5(pz - 1), s0 = ring5(pz), sp = ring5(pz + 1);
-        for (int i = tid; i < kNX * kNY; i += kThreads) {
-            const int nxh = i % kNX, nyh = i / kNX;
-            float gx, gy, gz;
-            grad(S.phiZ, nxh + 1, nyh + 1, sm, s0, sp, gx, gy, gz);
-            const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
-            const float inv = __frcp_rn(ind + 1e-9f); // = 1 / (ind + 1e-9), correctly rounded
-            S.nrm[s][0][nyh][nxh] = gx * inv;
-            S.nrm[s][1][nyh][nxh] = gy * inv;
-            S.nrm[s][2][nyh][nxh] = gz * inv;
-            S.nrm[s][3][nyh][nxh] = ind;
+        const int s = ringN(pz);
+        const int sm = ringP(pz - 1), s0 = ringP(pz), sp = ringP(pz + 1);
+        nrm_elem(S, s, sm, s0, sp, tid % kTX + 1, tid / kTX + 1);
+        if (tid < kNrmBorder) {
+            int nxh, nyh;
+            nrm_border_pos(tid, nxh, nyh);
+            nrm_elem(S, s, sm, s0, sp, nxh, nyh);
         }
     }
 
@@ -303,7 +361,7 @@ struct Bulk {
     // update reads 4 normal values instead of the full 3 x 3 x 3 stencil.
     static __device__ __forceinline__ void plane_terms(const BulkSmem &S, int pz, int tx, int ty, float &C,
                                                        float &Sv, float &Zv) {
-        const int s = ring2(pz);
+        const int s = ringN(pz);
         const int cx = tx + 1, cy = ty + 1;
         auto nx = [&](int dx, int dy) { return S.nrm[s][0][cy + dy][cx + dx]; };
         auto ny = [&](int dx, int dy) { return S.nrm[s][1][cy + dy][cx + dx]; };
@@ -362,7 +420,7 @@ struct Bulk {
         // div is the normal divergence of this cell, from the plane terms
         const int hx = tx + 2, hy = ty + 2; // phi ring centre
         const int nxh = tx + 1, nyh = ty + 1; // normal ring centre
-        const int s0 = ring2(z);
+        const int s0 = ringN(z);
         auto nat = [&](int comp) -> float { return S.nrm[s0][comp][nyh][nxh]; };
         const float curvature = 3.0f * div;
         const float sigma = a.clo_cs ? P.sigma * a.clo_cs[c0] : P.sigma;
@@ -380,14 +438,14 @@ struct Bulk {
         float nx = nat(0), ny = nat(1), nz = nat(2);
         if (near_ghost) {
             float gx, gy, gz;
-            grad(S.phiR, hx, hy, ring5(z - 1), ring5(z), ring5(z + 1), gx, gy, gz);
+            grad(S.phiR, hx, hy, ringP(z - 1), ringP(z), ringP(z + 1), gx, gy, gz);
             const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
             const float inv = __frcp_rn(ind + 1e-9f);
             nx = gx * inv;
             ny = gy * inv;
             nz = gz * inv;
         }
-        const float phi = S.phiR[ring5(z)][hy][hx];
+        const float phi = S.phiR[ringP(z)][hy][hx];
 
         // ---- gather f^n (after the stencil work, so that the Q values are live
         // only across the moments and the collision).  The source of direction q
