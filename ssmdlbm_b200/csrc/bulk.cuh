@@ -247,7 +247,9 @@ struct Bulk {
         const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
         for (int p = zs - 2; p <= zs + 3; ++p) fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
-        for (int p = zs - 1; p <= zs + 1; ++p) fill_nrm(S, p, tid);
+        GradCarry gc;
+        gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
+        for (int p = zs - 1; p <= zs + 1; ++p) fill_nrm_carry(S, p, tid, gc);
         __syncthreads();
         Curv cv;
         cv.start(S, zs, tx, ty);
@@ -255,7 +257,7 @@ struct Bulk {
         for (int z = zs; z < ze; ++z) {
             const float div = cv.advance(S, z, tx, ty);
             if (active) cell(a, S, x, y, z, tx, ty, div);
-            if (z + 2 <= ze) fill_nrm(S, z + 2, tid);
+            if (z + 2 <= ze) fill_nrm_carry(S, z + 2, tid, gc);
             if (z + 4 <= ze + 1) fill_phi(a, S, x0, y0, z + 4, tid);
             __syncthreads();
         }
@@ -298,10 +300,11 @@ struct Bulk {
             constexpr int q = 2 * k + 1;
             constexpr int cx = cx27(q), cy = cy27(q), cz = cz27(q);
             constexpr float w = (q <= 6) ? VS<Q>::w1 : (q <= 18 ? VS<Q>::w2 : VS<Q>::w3);
-            const float d = w * (at(cx, cy, cz) - at(-cx, -cy, -cz));
-            if constexpr (cx != 0) sx += cx > 0 ? d : -d;
-            if constexpr (cy != 0) sy += cy > 0 ? d : -d;
-            if constexpr (cz != 0) sz += cz > 0 ? d : -d;
+            // explicit fused forms: every instantiation rounds alike
+            const float d = at(cx, cy, cz) - at(-cx, -cy, -cz);
+            if constexpr (cx != 0) sx = fmaf(cx > 0 ? w : -w, d, sx);
+            if constexpr (cy != 0) sy = fmaf(cy > 0 ? w : -w, d, sy);
+            if constexpr (cz != 0) sz = fmaf(cz > 0 ? w : -w, d, sz);
         });
         gx = 3.0f * sx;
         gy = 3.0f * sy;
@@ -326,10 +329,11 @@ struct Bulk {
         }
     }
 
-    static __device__ __forceinline__ void nrm_elem(BulkSmem &S, int s, int sm, int s0, int sp, int nxh, int nyh) {
-        float gx, gy, gz;
-        grad(S.phiZ, nxh + 1, nyh + 1, sm, s0, sp, gx, gy, gz);
-        const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
+
+    // Normal, |grad phi| of one ring element from its gradient.
+    static __device__ __forceinline__ void store_nrm(BulkSmem &S, int s, int nxh, int nyh, float gx, float gy,
+                                                     float gz) {
+        const float ind = sqrtf(fmaf(gx, gx, fmaf(gy, gy, gz * gz)));
         const float inv = __frcp_rn(ind + 1e-9f); // = 1 / (ind + 1e-9), correctly rounded
         S.nrm[s][0][nyh][nxh] = gx * inv;
         S.nrm[s][1][nyh][nxh] = gy * inv;
@@ -337,12 +341,98 @@ struct Bulk {
         S.nrm[s][3][nyh][nxh] = ind;
     }
 
-    // Normals and |grad phi| of plane pz over the tile + 1-cell halo.
-    static __device__ void fill_nrm(BulkSmem &S, int pz, int tid) {
+    static __device__ __forceinline__ void nrm_elem(BulkSmem &S, int s, int sm, int s0, int sp, int nxh, int nyh) {
+        float gx, gy, gz;
+        grad(S.phiZ, nxh + 1, nyh + 1, sm, s0, sp, gx, gy, gz);
+        store_nrm(S, s, nxh, nyh, gx, gy, gz);
+    }
+
+    // Gradient of phi along the thread's own column from in-plane partial sums
+    // carried from plane to plane.  With the stencil weights of the velocity
+    // set the isotropic gradient 3 sum_q w_q c_q phi(x + c_q)
+    // (phaseField.cuh:158-218) splits by planes:
+    //   D3Q27, w = b(c_x) b(c_y) b(c_z) / 216 with b(0) = 4, b(+-1) = 1:
+    //     g_x(p) = 3/216 [Gx(p-1) + 4 Gx(p) + Gx(p+1)],  Gx = D_x S_y phi
+    //     g_y(p) = 3/216 [Gy(p-1) + 4 Gy(p) + Gy(p+1)],  Gy = D_y S_x phi
+    //     g_z(p) = 3/216 [Sxy(p+1) - Sxy(p-1)],          Sxy = S_x S_y phi
+    //   D3Q19, w = 2/36 on the faces and 1/36 on the edges:
+    //     g_x(p) = 3/36 [Cx(p) + Ax(p-1) + Ax(p+1)],  Ax = D_x phi,
+    //              Cx = 2 Ax + D_x phi(y + 1) + D_x phi(y - 1)  (same for y)
+    //     g_z(p) = 3/36 [T(p+1) - T(p-1)],  T = 2 phi + the 4 in-plane neighbours
+    // where S is the 1-4-1 sum and D the central difference along one axis.
+    // Each plane's 3 x 3 neighbourhood is read once (9 loads, not 18 / 26).
+    struct GradCarry {
+        float px, py, pz;          // plane p - 1: Gx, Gy, Sxy (D3Q27) / Ax, Ay, T (D3Q19)
+        float cx, cy, cz, ccx, ccy; // plane p: the same, and Cx, Cy (D3Q19)
+
+        // partials of ring plane P at ring position (hx, hy)
+        static __device__ __forceinline__ void partials(const float (&P)[kHY][kHX], int hx, int hy, float &a,
+                                                        float &b, float &c, float &d, float &e) {
+            auto f = [&](int i, int j) { return P[hy + j][hx + i]; };
+            if constexpr (Q == 27) {
+                const float sym = fmaf(4.0f, f(-1, 0), f(-1, -1) + f(-1, 1));
+                const float sy0 = fmaf(4.0f, f(0, 0), f(0, -1) + f(0, 1));
+                const float syp = fmaf(4.0f, f(1, 0), f(1, -1) + f(1, 1));
+                const float sxm = fmaf(4.0f, f(0, -1), f(-1, -1) + f(1, -1));
+                const float sxp = fmaf(4.0f, f(0, 1), f(-1, 1) + f(1, 1));
+                a = syp - sym;
+                b = sxp - sxm;
+                c = fmaf(4.0f, sy0, sym + syp);
+                d = e = 0.0f;
+            } else {
+                a = f(1, 0) - f(-1, 0);
+                b = f(0, 1) - f(0, -1);
+                c = fmaf(2.0f, f(0, 0), (f(1, 0) + f(-1, 0)) + (f(0, 1) + f(0, -1)));
+                d = fmaf(2.0f, a, (f(1, 1) - f(-1, 1)) + (f(1, -1) - f(-1, -1)));
+                e = fmaf(2.0f, b, (f(1, 1) - f(1, -1)) + (f(-1, 1) - f(-1, -1)));
+            }
+        }
+        // planes p - 1 and p enter (ring planes Pm, P0)
+        __device__ __forceinline__ void start(const float (&Pm)[kHY][kHX], const float (&P0)[kHY][kHX], int hx,
+                                              int hy) {
+            float d, e;
+            partials(Pm, hx, hy, px, py, pz, d, e);
+            partials(P0, hx, hy, cx, cy, cz, ccx, ccy);
+        }
+        // plane p + 1 enters: gradient at plane p
+        __device__ __forceinline__ void advance(const float (&Pp)[kHY][kHX], int hx, int hy, float &gx, float &gy,
+                                                float &gz) {
+            float a, b, c, d, e;
+            partials(Pp, hx, hy, a, b, c, d, e);
+            if constexpr (Q == 27) {
+                constexpr float k = float(3.0 / 216.0);
+                gx = k * fmaf(4.0f, cx, px + a);
+                gy = k * fmaf(4.0f, cy, py + b);
+                gz = k * (c - pz);
+            } else {
+                constexpr float k = float(3.0 / 36.0);
+                gx = k * (ccx + (px + a));
+                gy = k * (ccy + (py + b));
+                gz = k * (c - pz);
+            }
+            px = cx;
+            py = cy;
+            pz = cz;
+            cx = a;
+            cy = b;
+            cz = c;
+            ccx = d;
+            ccy = e;
+        }
+    };
+
+    // Normals and |grad phi| of plane pz over the tile + 1-cell halo: the
+    // thread's own column from its carried partial sums (planes pz - 1 and pz
+    // in gc; plane pz + 1 must be in the phi ring), the border element (tid <
+    // kNrmBorder) from the full stencil.
+    static __device__ void fill_nrm_carry(BulkSmem &S, int pz, int tid, GradCarry &gc) {
         const int s = ringN(pz);
-        const int sm = ringP(pz - 1), s0 = ringP(pz), sp = ringP(pz + 1);
-        nrm_elem(S, s, sm, s0, sp, tid % kTX + 1, tid / kTX + 1);
+        const int tx = tid % kTX, ty = tid / kTX;
+        float gx, gy, gz;
+        gc.advance(S.phiZ[ringP(pz + 1)], tx + 2, ty + 2, gx, gy, gz);
+        store_nrm(S, s, tx + 1, ty + 1, gx, gy, gz);
         if (tid < kNrmBorder) {
+            const int sm = ringP(pz - 1), s0 = ringP(pz), sp = ringP(pz + 1);
             int nxh, nyh;
             nrm_border_pos(tid, nxh, nyh);
             nrm_elem(S, s, sm, s0, sp, nxh, nyh);
@@ -439,7 +529,7 @@ struct Bulk {
         if (near_ghost) {
             float gx, gy, gz;
             grad(S.phiR, hx, hy, ringP(z - 1), ringP(z), ringP(z + 1), gx, gy, gz);
-            const float ind = sqrtf(gx * gx + gy * gy + gz * gz);
+            const float ind = sqrtf(fmaf(gx, gx, fmaf(gy, gy, gz * gz)));
             const float inv = __frcp_rn(ind + 1e-9f);
             nx = gx * inv;
             ny = gy * inv;
@@ -511,7 +601,7 @@ struct Bulk {
         const Moments m = moments<Q>(f, fx, fy, fz);
         float nu = fmaf(phi, P.nu_oil_minus_water, P.nu_water);
         if (a.clo_nut) nu += a.clo_nut[c0];
-        const float omega = __frcp_rn(0.5f + 3.0f * nu); // = 1 / (...), correctly rounded
+        const float omega = __frcp_rn(fmaf(3.0f, nu, 0.5f)); // = 1 / (0.5 + 3 nu), correctly rounded
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
         unroll<0, Q>([&](auto q) { Store<TF>::st(a.fq_dst[q] + c0, fo[q]); });
@@ -520,9 +610,10 @@ struct Bulk {
         const float sharp = P.gamma * phi * (1.0f - phi);
         float go[7];
         go[0] = kW7_0 * phi;
-        const float ax = 4.0f * phi * m.ux + sharp * nx;
-        const float ay = 4.0f * phi * m.uy + sharp * ny;
-        const float az = 4.0f * phi * m.uz + sharp * nz;
+        const float phi4 = 4.0f * phi;
+        const float ax = fmaf(phi4, m.ux, sharp * nx);
+        const float ay = fmaf(phi4, m.uy, sharp * ny);
+        const float az = fmaf(phi4, m.uz, sharp * nz);
         go[1] = kW7_1 * (phi + ax);
         go[2] = kW7_1 * (phi - ax);
         go[3] = kW7_1 * (phi + ay);
@@ -532,7 +623,7 @@ struct Bulk {
         if (bgk) {
             // BGK with the anti-diffusion flux inside the equilibrium; omega_g = 1
             // reduces to the reference's g = g_eq + h.
-            unroll<0, 7>([&](auto q) { go[q] = gin[q] + P.omega_g * (go[q] - gin[q]); });
+            unroll<0, 7>([&](auto q) { go[q] = fmaf(P.omega_g, go[q] - gin[q], gin[q]); });
         }
         unroll<0, 7>([&](auto q) { Store<TG>::st(a.gq_dst[q] + c0, go[q]); });
 
@@ -614,8 +705,10 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
         issue(zs);
         for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
-        B::fill_nrm(S, zs - 1, tid);
-        B::fill_nrm(S, zs, tid);
+        typename B::GradCarry gc;
+        gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
+        B::fill_nrm_carry(S, zs - 1, tid, gc);
+        B::fill_nrm_carry(S, zs, tid, gc);
         __syncthreads();
         typename B::Curv cv;
         cv.start(S, zs, tx, ty);
@@ -624,7 +717,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
         for (int z = zs; z < ze; ++z) {
             const int k = z - zs;
             issue(z + 1);
-            B::fill_nrm(S, z + 1, tid);
+            B::fill_nrm_carry(S, z + 1, tid, gc);
             if (tid == 0) {
                 if (!mbar_wait_bounded(&bars[k & 1], (uint32_t)(k >> 1) & 1u, kTmaWaitNs)) *abort_flag = 1;
                 else ++consumed;
@@ -698,14 +791,16 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
             issue(p + 2);
         }
         if (ok) {
-            B::fill_nrm(S, zs - 1, tid);
-            B::fill_nrm(S, zs, tid);
+            typename B::GradCarry gc;
+            gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
+            B::fill_nrm_carry(S, zs - 1, tid, gc);
+            B::fill_nrm_carry(S, zs, tid, gc);
             __syncthreads();
             typename B::Curv cv;
             cv.start(S, zs, tx, ty);
             __syncthreads();
             for (int z = zs; z < ze; ++z) {
-                B::fill_nrm(S, z + 1, tid);
+                B::fill_nrm_carry(S, z + 1, tid, gc);
                 const bool more = z + 1 < ze;
                 if (more) poll(z + 3);
                 __syncthreads();

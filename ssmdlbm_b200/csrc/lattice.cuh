@@ -160,17 +160,20 @@ __device__ __forceinline__ Moments moments(const float (&f)[Q], float fx, float 
     m.rho = s + 1.0f;
     const float inv = __frcp_rn(m.rho); // = 1 / rho, correctly rounded
     const float hinv = 0.5f * inv;
-    m.ux = jx * inv + fx * hinv;
-    m.uy = jy * inv + fy * hinv;
-    m.uz = jz * inv + fz * hinv;
+    m.ux = fmaf(jx, inv, fx * hinv);
+    m.uy = fmaf(jy, inv, fy * hinv);
+    m.uz = fmaf(jz, inv, fz * hinv);
     // T = sum f c c - rho u u + (u F + F u)/2; the (rho - 1) cs2 delta term
-    // of sum f_eq c c drops out of the traceless part.
-    const float txx = sxx - m.rho * m.ux * m.ux + m.ux * fx;
-    const float tyy = syy - m.rho * m.uy * m.uy + m.uy * fy;
-    const float tzz = szz - m.rho * m.uz * m.uz + m.uz * fz;
-    m.pxy = sxy - m.rho * m.ux * m.uy + 0.5f * (m.ux * fy + m.uy * fx);
-    m.pxz = sxz - m.rho * m.ux * m.uz + 0.5f * (m.ux * fz + m.uz * fx);
-    m.pyz = syz - m.rho * m.uy * m.uz + 0.5f * (m.uy * fz + m.uz * fy);
+    // of sum f_eq c c drops out of the traceless part.  (Here and below every
+    // multiply-add is written as an explicit fma, so that each instantiation
+    // of this code rounds alike.)
+    const float nrux = -m.rho * m.ux, nruy = -m.rho * m.uy;
+    const float txx = fmaf(m.ux, fx, fmaf(nrux, m.ux, sxx));
+    const float tyy = fmaf(m.uy, fy, fmaf(nruy, m.uy, syy));
+    const float tzz = fmaf(m.uz, fz, fmaf(-m.rho * m.uz, m.uz, szz));
+    m.pxy = fmaf(0.5f, fmaf(m.ux, fy, m.uy * fx), fmaf(nrux, m.uy, sxy));
+    m.pxz = fmaf(0.5f, fmaf(m.ux, fz, m.uz * fx), fmaf(nrux, m.uz, sxz));
+    m.pyz = fmaf(0.5f, fmaf(m.uy, fz, m.uz * fy), fmaf(nruy, m.uz, syz));
     const float tr = (txx + tyy + tzz) * kCs2;
     m.pxx = txx - tr;
     m.pyy = tyy - tr;
@@ -178,7 +181,7 @@ __device__ __forceinline__ Moments moments(const float (&f)[Q], float fx, float 
     return m;
 }
 
-// D3Q27: the post-collision populations of collide() evaluated as a polynomial in the
+// D3Q27 collide(): the post-collision populations evaluated as a polynomial in the
 // velocity components.  f_q - w_q = w_q P(c_q) with
 //   P(c) = sum_{a,b,c <= 2} p_abc c_x^a c_y^b c_z^c
 // (c_i^3 = c_i on the lattice), whose 17 nonzero coefficients collect the
@@ -191,37 +194,37 @@ __device__ __forceinline__ void collide27_tensor(const Moments &m, float omco, f
     const float ux = m.ux, uy = m.uy, uz = m.uz, rho = m.rho;
     const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
     const float uu = 1.5f * (ux2 + uy2 + uz2);
-    const float uF = ux * fx + uy * fy + uz * fz;
+    const float uF = fmaf(ux, fx, fmaf(uy, fy, uz * fz));
     const float trP = m.pxx + m.pyy + m.pzz; // ~0, kept for fidelity
     const float k45 = 4.5f * omco, k3 = 3.0f * k45;
     const float rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
     // 3rd-order Hermite coefficients of u (x) Pi (D3Q27.cuh:178-184)
-    const float axxy = m.pxx * uy + 2.0f * ux * m.pxy;
-    const float axxz = m.pxx * uz + 2.0f * ux * m.pxz;
-    const float ayyx = m.pyy * ux + 2.0f * uy * m.pxy;
-    const float ayyz = m.pyy * uz + 2.0f * uy * m.pyz;
-    const float azzx = m.pzz * ux + 2.0f * uz * m.pxz;
-    const float azzy = m.pzz * uy + 2.0f * uz * m.pyz;
-    const float axyz = ux * m.pyz + uy * m.pxz + uz * m.pxy;
+    const float axxy = fmaf(m.pxx, uy, 2.0f * ux * m.pxy);
+    const float axxz = fmaf(m.pxx, uz, 2.0f * ux * m.pxz);
+    const float ayyx = fmaf(m.pyy, ux, 2.0f * uy * m.pxy);
+    const float ayyz = fmaf(m.pyy, uz, 2.0f * uy * m.pyz);
+    const float azzx = fmaf(m.pzz, ux, 2.0f * uz * m.pxz);
+    const float azzy = fmaf(m.pzz, uy, 2.0f * uz * m.pyz);
+    const float axyz = fmaf(ux, m.pyz, fmaf(uy, m.pxz, uz * m.pxy));
     // coefficients: constant, linear (equilibrium + Guo + the linear parts of
     // the cubic terms), quadratic, mixed quadratic, cubic
-    const float p000 = rho * (1.0f - uu) - 1.0f - 1.5f * uF - k45 * kCs2 * trP;
-    const float p100 = 3.0f * rux + 1.5f * fx - 4.5f * rux * (uy2 + uz2) - k45 * (ayyx + azzx);
-    const float p010 = 3.0f * ruy + 1.5f * fy - 4.5f * ruy * (ux2 + uz2) - k45 * (axxy + azzy);
-    const float p001 = 3.0f * ruz + 1.5f * fz - 4.5f * ruz * (ux2 + uy2) - k45 * (axxz + ayyz);
-    const float p200 = 4.5f * ux * (rux + fx) + k45 * m.pxx;
-    const float p020 = 4.5f * uy * (ruy + fy) + k45 * m.pyy;
-    const float p002 = 4.5f * uz * (ruz + fz) + k45 * m.pzz;
-    const float p110 = 9.0f * rux * uy + 2.0f * k45 * m.pxy + 4.5f * (ux * fy + uy * fx);
-    const float p101 = 9.0f * rux * uz + 2.0f * k45 * m.pxz + 4.5f * (ux * fz + uz * fx);
-    const float p011 = 9.0f * ruy * uz + 2.0f * k45 * m.pyz + 4.5f * (uy * fz + uz * fy);
-    const float p210 = 13.5f * rux * ux * uy + k3 * axxy; // c_x^2 c_y
-    const float p201 = 13.5f * rux * ux * uz + k3 * axxz; // c_x^2 c_z
-    const float p120 = 13.5f * ruy * uy * ux + k3 * ayyx; // c_x c_y^2
-    const float p021 = 13.5f * ruy * uy * uz + k3 * ayyz; // c_y^2 c_z
-    const float p102 = 13.5f * ruz * uz * ux + k3 * azzx; // c_x c_z^2
-    const float p012 = 13.5f * ruz * uz * uy + k3 * azzy; // c_y c_z^2
-    const float p111 = 27.0f * rux * uy * uz + 2.0f * k3 * axyz;
+    const float p000 = fmaf(rho, 1.0f - uu, -1.0f) - fmaf(1.5f, uF, k45 * kCs2 * trP);
+    const float p100 = fmaf(3.0f, rux, 1.5f * fx) - fmaf(4.5f * rux, uy2 + uz2, k45 * (ayyx + azzx));
+    const float p010 = fmaf(3.0f, ruy, 1.5f * fy) - fmaf(4.5f * ruy, ux2 + uz2, k45 * (axxy + azzy));
+    const float p001 = fmaf(3.0f, ruz, 1.5f * fz) - fmaf(4.5f * ruz, ux2 + uy2, k45 * (axxz + ayyz));
+    const float p200 = fmaf(4.5f * ux, rux + fx, k45 * m.pxx);
+    const float p020 = fmaf(4.5f * uy, ruy + fy, k45 * m.pyy);
+    const float p002 = fmaf(4.5f * uz, ruz + fz, k45 * m.pzz);
+    const float p110 = fmaf(9.0f * rux, uy, fmaf(2.0f * k45, m.pxy, 4.5f * fmaf(ux, fy, uy * fx)));
+    const float p101 = fmaf(9.0f * rux, uz, fmaf(2.0f * k45, m.pxz, 4.5f * fmaf(ux, fz, uz * fx)));
+    const float p011 = fmaf(9.0f * ruy, uz, fmaf(2.0f * k45, m.pyz, 4.5f * fmaf(uy, fz, uz * fy)));
+    const float p210 = fmaf(13.5f * rux * ux, uy, k3 * axxy); // c_x^2 c_y
+    const float p201 = fmaf(13.5f * rux * ux, uz, k3 * axxz); // c_x^2 c_z
+    const float p120 = fmaf(13.5f * ruy * uy, ux, k3 * ayyx); // c_x c_y^2
+    const float p021 = fmaf(13.5f * ruy * uy, uz, k3 * ayyz); // c_y^2 c_z
+    const float p102 = fmaf(13.5f * ruz * uz, ux, k3 * azzx); // c_x c_z^2
+    const float p012 = fmaf(13.5f * ruz * uz, uy, k3 * azzy); // c_y c_z^2
+    const float p111 = fmaf(27.0f * rux * uy, uz, 2.0f * k3 * axyz);
 
     // z sweep: L_ab(cz) = sum_c p_abc cz^c, [cz + 1]
     float L00[3], L10[3], L01[3], L20[3], L02[3], L11[3];
@@ -262,37 +265,19 @@ __device__ __forceinline__ void collide27_tensor(const Moments &m, float omco, f
     });
 }
 
-// Post-collision shifted populations:
-//   f_q = f_eq(rho, u) + (1 - omega) f_neq^H(Pi, u) + F_q / 2
-// with the 2nd-order (D3Q19) or 3rd-order (D3Q27) Hermite forms of the
-// reference (D3Q19.cuh:133-177, D3Q27.cuh:147-201).  omco = 1 - omega.
-template <int Q>
-__device__ __forceinline__ void collide(const Moments &m, float omco, float fx, float fy, float fz,
-                                        float (&out)[Q]) {
-    if constexpr (Q == 27) {
-        collide27_tensor(m, omco, fx, fy, fz, out);
-        return;
-    }
+// D3Q19 collide(), by opposite pairs.
+__device__ __forceinline__ void collide19_pairs(const Moments &m, float omco, float fx, float fy, float fz,
+                                                float (&out)[19]) {
+    constexpr int Q = 19;
     const float ux = m.ux, uy = m.uy, uz = m.uz, rho = m.rho;
-    const float uu = 1.5f * (ux * ux + uy * uy + uz * uz);
-    const float uF = ux * fx + uy * fy + uz * fz;
+    const float uu = 1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+    const float uF = fmaf(ux, fx, fmaf(uy, fy, uz * fz));
     const float trP = m.pxx + m.pyy + m.pzz; // ~0, kept for fidelity
     const float k45 = 4.5f * omco;
     // part shared by every direction
-    const float A0 = rho * (1.0f - uu) - 1.0f - 1.5f * uF - k45 * kCs2 * trP;
+    const float A0 = fmaf(rho, 1.0f - uu, -1.0f) - fmaf(1.5f, uF, k45 * kCs2 * trP);
     out[0] = VS<Q>::w(0) * A0;
-
-    // 3rd-order Hermite coefficients of u (x) Pi (D3Q27.cuh:178-184)
-    float axxy = 0.f, axxz = 0.f, ayyx = 0.f, ayyz = 0.f, azzx = 0.f, azzy = 0.f, axyz = 0.f;
-    if constexpr (Q == 27) {
-        axxy = m.pxx * uy + 2.0f * ux * m.pxy;
-        axxz = m.pxx * uz + 2.0f * ux * m.pxz;
-        ayyx = m.pyy * ux + 2.0f * uy * m.pxy;
-        ayyz = m.pyy * uz + 2.0f * uy * m.pyz;
-        azzx = m.pzz * ux + 2.0f * uz * m.pxz;
-        azzy = m.pzz * uy + 2.0f * uz * m.pyz;
-        axyz = ux * m.pyz + uy * m.pxz + uz * m.pxy;
-    }
+    const float hrho = 0.5f * rho;
 
     unroll<0, (Q - 1) / 2>([&](auto k) {
         constexpr int qp = 2 * k + 1, qm = 2 * k + 2;
@@ -307,37 +292,28 @@ __device__ __forceinline__ void collide(const Moments &m, float omco, float fx, 
         if constexpr (cx != 0) pcc += m.pxx;
         if constexpr (cy != 0) pcc += m.pyy;
         if constexpr (cz != 0) pcc += m.pzz;
-        if constexpr (cx * cy != 0) pcc += (cx * cy > 0 ? 2.0f : -2.0f) * m.pxy;
-        if constexpr (cx * cz != 0) pcc += (cx * cz > 0 ? 2.0f : -2.0f) * m.pxz;
-        if constexpr (cy * cz != 0) pcc += (cy * cz > 0 ? 2.0f : -2.0f) * m.pyz;
+        if constexpr (cx * cy != 0) pcc = fmaf(cx * cy > 0 ? 2.0f : -2.0f, m.pxy, pcc);
+        if constexpr (cx * cz != 0) pcc = fmaf(cx * cz > 0 ? 2.0f : -2.0f, m.pxz, pcc);
+        if constexpr (cy * cz != 0) pcc = fmaf(cy * cz > 0 ? 2.0f : -2.0f, m.pyz, pcc);
         const float cu3 = 3.0f * cu; // reference "cu" = as2 (c.u)
-        float E = A0 + 0.5f * rho * cu3 * cu3 + k45 * pcc + 1.5f * cu3 * cF;
-        float O = rho * cu3 + 1.5f * cF;
-        if constexpr (Q == 27) {
-            O += rho * (cu3 * cu3 * cu3 * float(1.0 / 6.0) - uu * cu3);
-            float h3 = 0.f;
-            constexpr float t = 1.0f / 3.0f;
-            // (cx^2 cy - cy/3) etc., constant-folded per direction
-            constexpr float cxxy = float(cx * cx * cy) - float(cy) * t;
-            constexpr float cxxz = float(cx * cx * cz) - float(cz) * t;
-            constexpr float cyyx = float(cx * cy * cy) - float(cx) * t;
-            constexpr float cyyz = float(cy * cy * cz) - float(cz) * t;
-            constexpr float czzx = float(cx * cz * cz) - float(cx) * t;
-            constexpr float czzy = float(cy * cz * cz) - float(cy) * t;
-            constexpr float cxyz = float(cx * cy * cz);
-            if constexpr (cxxy != 0.f) h3 += cxxy * axxy;
-            if constexpr (cxxz != 0.f) h3 += cxxz * axxz;
-            if constexpr (cyyx != 0.f) h3 += cyyx * ayyx;
-            if constexpr (cyyz != 0.f) h3 += cyyz * ayyz;
-            if constexpr (czzx != 0.f) h3 += czzx * azzx;
-            if constexpr (czzy != 0.f) h3 += czzy * azzy;
-            float odd3 = 3.0f * h3;
-            if constexpr (cxyz != 0.f) odd3 += 6.0f * cxyz * axyz;
-            O += k45 * odd3;
-        }
+        const float cF15 = 1.5f * cF;
+        // E = A0 + 0.5 rho cu3^2 + k45 pcc + 1.5 cu3 cF, O = rho cu3 + 1.5 cF
+        const float E = fmaf(cu3, fmaf(hrho, cu3, cF15), fmaf(k45, pcc, A0));
+        const float O = fmaf(rho, cu3, cF15);
         out[qp] = w * (E + O);
         out[qm] = w * (E - O);
     });
+}
+
+// Post-collision shifted populations:
+//   f_q = f_eq(rho, u) + (1 - omega) f_neq^H(Pi, u) + F_q / 2
+// with the 2nd-order (D3Q19) or 3rd-order (D3Q27) Hermite forms of the
+// reference (D3Q19.cuh:133-177, D3Q27.cuh:147-201).  omco = 1 - omega.
+template <int Q>
+__device__ __forceinline__ void collide(const Moments &m, float omco, float fx, float fy, float fz,
+                                        float (&out)[Q]) {
+    if constexpr (Q == 27) collide27_tensor(m, omco, fx, fy, fz, out);
+    else collide19_pairs(m, omco, fx, fy, fz, out);
 }
 
 } // namespace ssmd
