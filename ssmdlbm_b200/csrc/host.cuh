@@ -179,8 +179,10 @@ inline void bulk_slots(int &per_sm, int &sms) {
     sms = cached_sms;
 }
 
-// Bulk tiling: 32 x 8 columns; the z chunk minimises (waves of work items) x
-// (planes per item + the 3-plane ring prologue) unless the caller fixes tile_z.
+// Bulk tiling: 32 x 8 columns.  Unless the caller fixes tile_z, the z chunk
+// is 16 planes (measured best on B200 for lattices of several waves: longer
+// chunks save ring prologues but lose more to the last wave), shortened on
+// small lattices until the work items fill every resident slot once.
 inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tiles_x, int &tiles_y,
                    int &zchunk, int &nchunks) {
     tiles_x = (int)((G.nx + kTX - 1) / kTX);
@@ -190,17 +192,8 @@ inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tile
     if (p.tile_z > 0) {
         zchunk = p.tile_z;
     } else {
-        double best = 1e300;
-        zchunk = nzf;
-        for (int zc = 4; zc <= nzf; ++zc) {
-            const long nch = (nzf + zc - 1) / zc;
-            const long waves = (cols * nch + slots - 1) / slots;
-            const double t = (double)waves * (zc + 3);
-            if (t < best * (1.0 - 1e-9)) {
-                best = t;
-                zchunk = zc;
-            }
-        }
+        zchunk = 16;
+        while (zchunk > 4 && cols * ((nzf + zchunk - 1) / zchunk) < slots) --zchunk;
     }
     if (zchunk > nzf) zchunk = nzf;
     nchunks = (nzf + zchunk - 1) / zchunk;
