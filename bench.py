@@ -312,6 +312,115 @@ def mlp_throughput(rows: int = 1 << 20, reps: int = 20):
     return res
 
 
+def jet_stats(sim) -> dict:
+    """Centreline u_z and phi (fluid planes), phi mass and droplets of the
+    fields the last step stored."""
+    uz, phi = sim.centreline()
+    d = sim.droplets()
+    return {"uz": uz[1:-1], "phi": phi[1:-1], "mass": sim.reduce(raise_unstable=False)["phi_sum_next"],
+            "droplets": int(len(d)), "droplet_volume": float(d["volume"].sum()) if len(d) else 0.0}
+
+
+def stat_diffs(s: dict, ref: dict) -> dict:
+    import numpy as np
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+    return {"centreline_uz": rel(s["uz"], ref["uz"]), "centreline_phi": rel(s["phi"], ref["phi"]),
+            "phi_mass": abs(s["mass"] - ref["mass"]) / max(abs(ref["mass"]), 1e-30),
+            "droplets": [s["droplets"], ref["droplets"]],
+            "droplet_volume": (abs(s["droplet_volume"] - ref["droplet_volume"]) / ref["droplet_volume"]
+                               if ref["droplet_volume"] > 0 else None)}
+
+
+def run_precision(steps: int = 5000):
+    """The 128 x 128 x 512 D3Q27 jet for `steps` steps with FP32, shifted FP16
+    and shifted BF16 population storage (FP32 arithmetic in all three): the
+    16-bit runs' centreline u_z, centreline phi, phi mass and droplets against
+    the FP32 run's."""
+    import torch
+    from ssmdlbm_b200 import _lib
+    from ssmdlbm_b200.lbm import Simulation
+    out, ref = {}, None
+    for name, stg in (("f32", _lib.STORAGE_F32), ("f16", _lib.STORAGE_F16), ("bf16", _lib.STORAGE_BF16)):
+        sim = Simulation(workload(stg, 27))
+        sim.init()
+        sim.step(steps, store_macros=True)
+        st = jet_stats(sim)
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+        if ref is None:
+            ref = st
+            out["f32"] = {"droplets": st["droplets"], "phi_mass": st["mass"]}
+        else:
+            out[name + "_vs_f32"] = stat_diffs(st, ref)
+    return {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, {steps} steps, nozzle 16, tau 0.52, seed 1",
+            "reference": "the FP32-storage run (same arithmetic); the FP64 oracle judges small lattices "
+                         "in tests/test_parity_gpu.py", **out}
+
+
+def run_production(net, steps: int = 200, update_every: int = 10):
+    """Production lattice 384 x 384 x 1536 (226 M cells, D3Q27 + D3Q7, nozzle
+    24, w 0.06 + 1 % noise, seed 3, sigma 1e-3, tau 0.52): FP16 storage with
+    the learned closure (network from the closure leg, refreshed every
+    `update_every` steps) against the plain FP32 method, `steps` steps each."""
+    import ctypes as ct
+    import torch
+    from ssmdlbm_b200 import _lib, configs
+    from ssmdlbm_b200.lbm import Simulation
+    L = _lib.lib()
+    peak, _ = hbm_peak()
+    res = {"workload": f"oil jet D3Q27+D3Q7 384x384x1536, nozzle 24, w 0.06 + 1% noise, seed 3, {steps} steps; "
+                       f"FP16 + closure every {update_every} steps vs FP32 plain"}
+    stats = {}
+    for name, stg in (("f32_plain", _lib.STORAGE_F32), ("f16_closure", _lib.STORAGE_F16)):
+        p = configs.oil_jet(384, 384, 1536, 27, tau=0.52, sigma=1e-3, width=4.0, mobility=0.1, diam=24,
+                            w_in=0.06, noise=0.01, seed=3, storage=stg)
+        sim = Simulation(p)
+        keep = None
+        if net is not None and name == "f16_closure":
+            n = sim.cells
+            nut = torch.zeros(n, device=sim.device)
+            cs = torch.ones(n, device=sim.device)
+            out = torch.empty(n, 2, device=sim.device)
+            feats = torch.empty(n, _lib.MLP_IN, device=sim.device)
+            cl = _lib.Closure(nut.data_ptr(), cs.data_ptr())
+            sim.p.closure = ct.addressof(cl)
+            keep = (nut, cs, out, feats, cl)
+        sim.init()
+        sim.step(2, store_macros=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sim.torch_stream)
+        i = 0
+        while i < steps:
+            j = min(update_every, steps - i)
+            if keep is not None:
+                nut, cs, out, feats, _ = keep
+                _lib.check(L.ssmd_closure_features(ct.byref(sim.p), ct.byref(sim.fields), feats.data_ptr(),
+                                                   sim.stream))
+                _lib.check(L.ssmd_closure_apply(ct.byref(sim.p), net.net.data_ptr(), feats.data_ptr(),
+                                                out.data_ptr(), nut.data_ptr(), cs.data_ptr(), 0.05, sim.stream))
+            sim.step(j, store_macros=True)
+            i += j
+        e1.record(sim.torch_stream)
+        e1.synchronize()
+        dt = e0.elapsed_time(e1) / 1e3
+        bm = bulk_launch_ms(sim, 10)
+        s_f = 4 if stg == _lib.STORAGE_F32 else 2
+        stats[name] = jet_stats(sim)
+        res[name] = {"mlups": round(sim.cells * steps / dt / 1e6, 1), "ms_per_step": round(dt * 1e3 / steps, 3),
+                     "bulk_ms": round(bm, 3),
+                     "roofline_frac": round(b_alg(27, s_f) * sim.cells / (bm * 1e-3) / 1e9 / peak, 4),
+                     "device_gb": round(torch.cuda.max_memory_allocated(sim.device) / 1e9, 1),
+                     "status": sim.check_status()}
+        sim.close()
+        del sim, keep
+        torch.cuda.empty_cache()
+        torch.cuda.reset_peak_memory_stats()
+    res["f16_closure_vs_f32_plain"] = stat_diffs(stats["f16_closure"], stats["f32_plain"])
+    res["time_ratio"] = round(res["f16_closure"]["ms_per_step"] / res["f32_plain"]["ms_per_step"], 4)
+    return res
+
+
 def run_closure(full: bool):
     """Coarse-plus-closure run against the fine run it learns from (D3Q19 oil
     jet, 2x coarsening).  Default: fine 128 x 128 x 512 for 4000 steps;
@@ -338,7 +447,7 @@ def run_closure(full: bool):
                                      "droplet_volume")},
         "heldout_loss": r["heldout_loss"], "samples": r["samples"], "mlp_status": r["mlp_status"],
         "mlp": mlp_throughput(),
-    }
+    }, r["net"]
 
 
 def run_ours(a, world, rank, local):
@@ -391,7 +500,9 @@ def run_ours(a, world, rank, local):
             torch.cuda.empty_cache()
 
     sweep = run_sweep() if not a.quick else None
-    closure_line = run_closure(a.closure_full) if (not a.quick and not a.no_closure) else None
+    closure_line, net = run_closure(a.closure_full) if (not a.quick and not a.no_closure) else (None, None)
+    precision = run_precision() if not a.quick else None
+    production = run_production(net) if (not a.quick and not a.no_production) else None
 
     p.bulk_path, p.tile_z = sim_path, sim_tz
     e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
@@ -422,6 +533,8 @@ def run_ours(a, world, rank, local):
         "variants": variants,
         "sweep": sweep,
         "closure": closure_line,
+        "precision": precision,
+        "production": production,
         "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
     }
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -474,6 +587,8 @@ def main() -> int:
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--no-production", action="store_true",
+                    help="skip the 384 x 384 x 1536 production-lattice leg")
     ap.add_argument("--closure-full", action="store_true",
                     help="closure leg at 256 x 256 x 1024, 20000 steps (minutes)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],

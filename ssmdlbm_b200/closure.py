@@ -363,5 +363,5 @@ def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train
         "errors_plain": stat_errors(plain, fine), "errors_closure": stat_errors(closed, fine),
         "heldout_loss": {"no_closure": loss_plain, "untrained": loss_before, "trained": loss_after},
         "train_curve": curve, "train_device_s": train_s, "samples": int(feats.shape[0]),
-        "wall_s": time.perf_counter() - t0, "mlp_status": net.status(),
+        "wall_s": time.perf_counter() - t0, "mlp_status": net.status(), "net": net,
     }
