@@ -34,7 +34,7 @@ struct BatchInst {
 };
 
 template <int Q, class T>
-__global__ void __launch_bounds__(kThreads, SSMD_BULK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, kBulkMinBlocks<Q>)
     bulk_batch_kernel(BatchHeader *hdr, const BatchInst<T> *inst, int parity, uint32_t flags) {
     using B = Bulk<Q, T, T>;
     __shared__ BulkSmem S;

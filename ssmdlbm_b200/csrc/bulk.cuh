@@ -28,9 +28,11 @@
 
 namespace ssmd {
 
-#ifndef SSMD_BULK_MIN_BLOCKS
-#define SSMD_BULK_MIN_BLOCKS 3 // resident work items per SM the register budget targets
-#endif
+// Resident work items per SM the register budget targets: 4 for D3Q19 (64
+// registers, its gradient carry in shared memory), 3 for D3Q27 (80 registers:
+// at 64 its 27 populations spill).
+template <int Q>
+constexpr int kBulkMinBlocks = Q == 19 ? 4 : 3;
 
 constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
 constexpr int kHX = kTX + 4, kHY = kTY + 4; // phi ring (halo 2)
@@ -70,6 +72,7 @@ struct BulkSmem {
     float phiR[6][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
     float phiZ[6][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
     float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
+    float carry[8][kThreads];  // D3Q19 gradient carry (GradCarry), one column per thread
 };
 
 // Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
@@ -247,7 +250,7 @@ struct Bulk {
         const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
         for (int p = zs - 2; p <= zs + 3; ++p) fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
-        GradCarry gc;
+        GradCarry gc(S, tid);
         gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
         for (int p = zs - 1; p <= zs + 1; ++p) fill_nrm_carry(S, p, tid, gc);
         __syncthreads();
@@ -361,9 +364,26 @@ struct Bulk {
     //     g_z(p) = 3/36 [T(p+1) - T(p-1)],  T = 2 phi + the 4 in-plane neighbours
     // where S is the 1-4-1 sum and D the central difference along one axis.
     // Each plane's 3 x 3 neighbourhood is read once (9 loads, not 18 / 26).
+    // The carried sums: plane p - 1: Gx, Gy, Sxy (D3Q27) / Ax, Ay, T (D3Q19);
+    // plane p: the same, and Cx, Cy (D3Q19).  D3Q27 keeps them in registers;
+    // D3Q19 keeps them in the thread's column of BulkSmem::carry, which frees
+    // the registers its 4-blocks-per-SM budget needs.
     struct GradCarry {
-        float px, py, pz;          // plane p - 1: Gx, Gy, Sxy (D3Q27) / Ax, Ay, T (D3Q19)
-        float cx, cy, cz, ccx, ccy; // plane p: the same, and Cx, Cy (D3Q19)
+        float reg[8];
+        float *col; // BulkSmem::carry[0] + tid (D3Q19)
+        __device__ __forceinline__ GradCarry(BulkSmem &S, int tid) : col(&S.carry[0][tid]) {}
+        __device__ __forceinline__ float &v(int k) {
+            if constexpr (Q == 27) return reg[k];
+            else return col[k * kThreads];
+        }
+        __device__ __forceinline__ float &px() { return v(0); }
+        __device__ __forceinline__ float &py() { return v(1); }
+        __device__ __forceinline__ float &pz() { return v(2); }
+        __device__ __forceinline__ float &cx() { return v(3); }
+        __device__ __forceinline__ float &cy() { return v(4); }
+        __device__ __forceinline__ float &cz() { return v(5); }
+        __device__ __forceinline__ float &ccx() { return v(6); }
+        __device__ __forceinline__ float &ccy() { return v(7); }
 
         // partials of ring plane P at ring position (hx, hy)
         static __device__ __forceinline__ void partials(const float (&P)[kHY][kHX], int hx, int hy, float &a,
@@ -390,9 +410,17 @@ struct Bulk {
         // planes p - 1 and p enter (ring planes Pm, P0)
         __device__ __forceinline__ void start(const float (&Pm)[kHY][kHX], const float (&P0)[kHY][kHX], int hx,
                                               int hy) {
-            float d, e;
-            partials(Pm, hx, hy, px, py, pz, d, e);
-            partials(P0, hx, hy, cx, cy, cz, ccx, ccy);
+            float a, b, c, d, e;
+            partials(Pm, hx, hy, a, b, c, d, e);
+            px() = a;
+            py() = b;
+            pz() = c;
+            partials(P0, hx, hy, a, b, c, d, e);
+            cx() = a;
+            cy() = b;
+            cz() = c;
+            ccx() = d;
+            ccy() = e;
         }
         // plane p + 1 enters: gradient at plane p
         __device__ __forceinline__ void advance(const float (&Pp)[kHY][kHX], int hx, int hy, float &gx, float &gy,
@@ -401,23 +429,23 @@ struct Bulk {
             partials(Pp, hx, hy, a, b, c, d, e);
             if constexpr (Q == 27) {
                 constexpr float k = float(3.0 / 216.0);
-                gx = k * fmaf(4.0f, cx, px + a);
-                gy = k * fmaf(4.0f, cy, py + b);
-                gz = k * (c - pz);
+                gx = k * fmaf(4.0f, cx(), px() + a);
+                gy = k * fmaf(4.0f, cy(), py() + b);
+                gz = k * (c - pz());
             } else {
                 constexpr float k = float(3.0 / 36.0);
-                gx = k * (ccx + (px + a));
-                gy = k * (ccy + (py + b));
-                gz = k * (c - pz);
+                gx = k * (ccx() + (px() + a));
+                gy = k * (ccy() + (py() + b));
+                gz = k * (c - pz());
             }
-            px = cx;
-            py = cy;
-            pz = cz;
-            cx = a;
-            cy = b;
-            cz = c;
-            ccx = d;
-            ccy = e;
+            px() = cx();
+            py() = cy();
+            pz() = cz();
+            cx() = a;
+            cy() = b;
+            cz() = c;
+            ccx() = d;
+            ccy() = e;
         }
     };
 
@@ -658,7 +686,7 @@ constexpr uint64_t kTmaWaitNs = 2000000000ull;
 // PATH: 1 = per-cell gathers, 2 = TMA boxes for the phi halo, 3 = TMA slabs
 // for the populations (phi halo by gathers).
 template <int Q, class TF, class TG, int PATH>
-__global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : kBulkMinBlocks<Q>)
     bulk_kernel(const StepArgs<TF, TG> a, const __grid_constant__ CUtensorMap gmap,
                 const __grid_constant__ CUtensorMap fmap) {
     using B = Bulk<Q, TF, TG>;
@@ -705,7 +733,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
         issue(zs);
         for (int p = zs - 2; p <= zs + 2; ++p) B::fill_phi(a, S, x0, y0, p, tid);
         __syncthreads();
-        typename B::GradCarry gc;
+        typename B::GradCarry gc(S, tid);
         gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
         B::fill_nrm_carry(S, zs - 1, tid, gc);
         B::fill_nrm_carry(S, zs, tid, gc);
@@ -791,7 +819,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : SSMD_BULK_MIN_BLOCKS
             issue(p + 2);
         }
         if (ok) {
-            typename B::GradCarry gc;
+            typename B::GradCarry gc(S, tid);
             gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
             B::fill_nrm_carry(S, zs - 1, tid, gc);
             B::fill_nrm_carry(S, zs, tid, gc);
