@@ -32,7 +32,7 @@ namespace ssmd {
 // registers, its gradient carry in shared memory), 3 for D3Q27 (80 registers:
 // at 64 its 27 populations spill).
 template <int Q>
-constexpr int kBulkMinBlocks = Q == 19 ? 4 : 3;
+constexpr int kBulkMinBlocks = 4;
 
 constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
 constexpr int kHX = kTX + 4, kHY = kTY + 4; // phi ring (halo 2)
@@ -69,10 +69,9 @@ struct Slab {
 };
 
 struct BulkSmem {
-    float phiR[6][kHY][kHX]; // phi as the reference's streamCollide sees it (ghost values kept)
     float phiZ[6][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
     float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
-    float carry[8][kThreads];  // D3Q19 gradient carry (GradCarry), one column per thread
+    float carry[11][kThreads]; // gradient and curvature carries, one column per thread
 };
 
 // Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
@@ -139,24 +138,18 @@ struct Bulk {
         }
     }
 
-    // phi of ring element (hx, hy) = lattice cell (rx, ry) before wrapping, plane gz.
+    // phi of ring element (hx, hy) = lattice cell (rx, ry) before wrapping,
+    // plane gz: fluid cells from g, ghost and outside cells 0 (the field
+    // computeForces sees, phaseField.cuh:118-142).
     static __device__ __forceinline__ void phi_elem(const A &a, BulkSmem &S, int s, int hx, int hy, int rx, int ry,
                                                     int gz, bool zfluid) {
         const Geometry &G = a.geo;
         const int gx = halo_axis(a, rx, G.nx, G.bcx == BC_PERIODIC);
         const int gy = halo_axis(a, ry, G.ny, G.bcy == BC_PERIODIC);
-        float raw = 0.f, zer = 0.f;
-        if (gx >= 0 && gy >= 0 && gz >= 0) {
-            const uint32_t c = cell_index(G, gx, gy, gz);
-            if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
-                raw = phi_from_g(a, gx, gy, gz, c);
-                zer = raw;
-            } else {
-                raw = a.fld.phi[c];
-            }
-        }
-        S.phiR[s][hy][hx] = raw;
-        S.phiZ[s][hy][hx] = zer;
+        float v = 0.f;
+        if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi)
+            v = phi_from_g(a, gx, gy, gz, cell_index(G, gx, gy, gz));
+        S.phiZ[s][hy][hx] = v;
     }
 
     // Fill ring slot of plane pz with phi over the tile + 2-cell halo.
@@ -164,7 +157,7 @@ struct Bulk {
         const Geometry &G = a.geo;
         const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
         const int s = ringP(pz);
-        const bool zfluid = gz >= G.z_lo && gz <= G.z_hi;
+        const bool zfluid = gz >= G.z_lo && gz <= G.z_hi; // (gz = -1 outside a non-periodic axis)
         const int tx = tid % kTX, ty = tid / kTX;
         phi_elem(a, S, s, tx + 2, ty + 2, x0 + tx, y0 + ty, gz, zfluid);
         if (tid < kPhiBorder) {
@@ -194,30 +187,23 @@ struct Bulk {
             const int rx = x0 - 2 + hx, ry = y0 - 2 + hy;
             const int gx = halo_axis(a, rx, G.nx, px);
             const int gy = halo_axis(a, ry, G.ny, py);
-            float raw = 0.f, zer = 0.f;
-            if (gx >= 0 && gy >= 0 && gz >= 0) {
-                const uint32_t c = cell_index(G, gx, gy, gz);
-                if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
-                    const bool edge = (px && (rx < 1 || rx > (int)G.nx - 2)) || (py && (ry < 1 || ry > (int)G.ny - 2));
-                    if (edge) {
-                        raw = phi_from_g(a, gx, gy, gz, c);
-                    } else {
-                        const int col = hy * GB::WX + hx + GB::XH - 2;
-                        raw = tofloat(B[0 * GB::BOX + col]);
-                        raw += tofloat(B[1 * GB::BOX + col - 1]);
-                        raw += tofloat(B[2 * GB::BOX + col + 1]);
-                        raw += tofloat(B[3 * GB::BOX + col]);
-                        raw += tofloat(B[4 * GB::BOX + col]);
-                        raw += tofloat(B[5 * GB::BOX + col]);
-                        raw += tofloat(B[6 * GB::BOX + col]);
-                    }
-                    zer = raw;
+            float v = 0.f;
+            if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi) {
+                const bool edge = (px && (rx < 1 || rx > (int)G.nx - 2)) || (py && (ry < 1 || ry > (int)G.ny - 2));
+                if (edge) {
+                    v = phi_from_g(a, gx, gy, gz, cell_index(G, gx, gy, gz));
                 } else {
-                    raw = a.fld.phi[c];
+                    const int col = hy * GB::WX + hx + GB::XH - 2;
+                    v = tofloat(B[0 * GB::BOX + col]);
+                    v += tofloat(B[1 * GB::BOX + col - 1]);
+                    v += tofloat(B[2 * GB::BOX + col + 1]);
+                    v += tofloat(B[3 * GB::BOX + col]);
+                    v += tofloat(B[4 * GB::BOX + col]);
+                    v += tofloat(B[5 * GB::BOX + col]);
+                    v += tofloat(B[6 * GB::BOX + col]);
                 }
             }
-            S.phiR[s][hy][hx] = raw;
-            S.phiZ[s][hy][hx] = zer;
+            S.phiZ[s][hy][hx] = v;
         }
     }
 
@@ -254,7 +240,7 @@ struct Bulk {
         gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
         for (int p = zs - 1; p <= zs + 1; ++p) fill_nrm_carry(S, p, tid, gc);
         __syncthreads();
-        Curv cv;
+        Curv cv(S, tid);
         cv.start(S, zs, tx, ty);
         __syncthreads();
         for (int z = zs; z < ze; ++z) {
@@ -294,10 +280,17 @@ struct Bulk {
     template <class Ring>
     static __device__ __forceinline__ void grad(const Ring &R, int hx, int hy, int sm, int s0, int sp,
                                                 float &gx, float &gy, float &gz) {
-        auto at = [&](int dx, int dy, int dz) -> float {
-            const int sl = dz < 0 ? sm : (dz > 0 ? sp : s0);
-            return R[sl][hy + dy][hx + dx];
-        };
+        grad_at(
+            [&](int dx, int dy, int dz) -> float {
+                const int sl = dz < 0 ? sm : (dz > 0 ? sp : s0);
+                return R[sl][hy + dy][hx + dx];
+            },
+            gx, gy, gz);
+    }
+
+    // The same gradient of the field phi(dx, dy, dz) around the centre.
+    template <class At>
+    static __device__ __forceinline__ void grad_at(At &&at, float &gx, float &gy, float &gz) {
         float sx = 0.f, sy = 0.f, sz = 0.f;
         unroll<0, (Q - 1) / 2>([&](auto k) {
             constexpr int q = 2 * k + 1;
@@ -373,8 +366,7 @@ struct Bulk {
         float *col; // BulkSmem::carry[0] + tid (D3Q19)
         __device__ __forceinline__ GradCarry(BulkSmem &S, int tid) : col(&S.carry[0][tid]) {}
         __device__ __forceinline__ float &v(int k) {
-            if constexpr (Q == 27) return reg[k];
-            else return col[k * kThreads];
+            return col[k * kThreads];
         }
         __device__ __forceinline__ float &px() { return v(0); }
         __device__ __forceinline__ float &py() { return v(1); }
@@ -502,24 +494,29 @@ struct Bulk {
     // Per-thread curvature state along the column: C of the current plane and
     // S - Z of the current and previous planes.
     struct Curv {
-        float prev_d, cur_c, cur_d;
+        float *col;
+        __device__ __forceinline__ Curv(BulkSmem &S, int tid) : col(&S.carry[8][tid]) {}
+        __device__ __forceinline__ float &prev_d() { return col[0]; }
+        __device__ __forceinline__ float &cur_c() { return col[kThreads]; }
+        __device__ __forceinline__ float &cur_d() { return col[2 * kThreads]; }
         // planes zs - 1 and zs must be in the normal ring; ends before any
         // thread may overwrite plane zs - 1 (the caller's next barrier)
         __device__ __forceinline__ void start(const BulkSmem &S, int zs, int tx, int ty) {
             float c, sv, zv;
             plane_terms(S, zs - 1, tx, ty, c, sv, zv);
-            prev_d = sv - zv;
-            plane_terms(S, zs, tx, ty, cur_c, sv, zv);
-            cur_d = sv - zv;
+            prev_d() = sv - zv;
+            plane_terms(S, zs, tx, ty, c, sv, zv);
+            cur_c() = c;
+            cur_d() = sv - zv;
         }
         // plane z + 1 just entered the ring: returns the divergence at plane z
         __device__ __forceinline__ float advance(const BulkSmem &S, int z, int tx, int ty) {
             float c, sv, zv;
             plane_terms(S, z + 1, tx, ty, c, sv, zv);
-            const float div = cur_c + (sv + zv) + prev_d;
-            prev_d = cur_d;
-            cur_c = c;
-            cur_d = sv - zv;
+            const float div = cur_c() + (sv + zv) + prev_d();
+            prev_d() = cur_d();
+            cur_c() = c;
+            cur_d() = sv - zv;
             return div;
         }
     };
@@ -555,15 +552,25 @@ struct Bulk {
                                 (!pz && (z <= G.z_lo || z >= G.z_hi));
         float nx = nat(0), ny = nat(1), nz = nat(2);
         if (near_ghost) {
+            // phi with ghost values: the ring's for fluid cells, the phi array
+            // (written by the boundaries, constant during this kernel) for ghost
+            // cells, 0 outside the lattice
+            auto raw = [&](int dx, int dy, int dz) -> float {
+                const int gx = axis_nb(x + dx, (int)G.nx, px), gy = axis_nb(y + dy, (int)G.ny, py);
+                const int gz = axis_nb(z + dz, (int)G.nz, pz);
+                if (gx < 0 || gy < 0 || gz < 0) return 0.f;
+                if (fluid(G, gx, gy, gz)) return S.phiZ[ringP(z + dz)][hy + dy][hx + dx];
+                return a.fld.phi[cell_index(G, gx, gy, gz)];
+            };
             float gx, gy, gz;
-            grad(S.phiR, hx, hy, ringP(z - 1), ringP(z), ringP(z + 1), gx, gy, gz);
+            grad_at(raw, gx, gy, gz);
             const float ind = sqrtf(fmaf(gx, gx, fmaf(gy, gy, gz * gz)));
             const float inv = __frcp_rn(ind + 1e-9f);
             nx = gx * inv;
             ny = gy * inv;
             nz = gz * inv;
         }
-        const float phi = S.phiR[ringP(z)][hy][hx];
+        const float phi = S.phiZ[ringP(z)][hy][hx];
 
         // ---- gather f^n (after the stencil work, so that the Q values are live
         // only across the moments and the collision).  The source of direction q
@@ -738,7 +745,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : kBulkMinBlocks<Q>)
         B::fill_nrm_carry(S, zs - 1, tid, gc);
         B::fill_nrm_carry(S, zs, tid, gc);
         __syncthreads();
-        typename B::Curv cv;
+        typename B::Curv cv(S, tid);
         cv.start(S, zs, tx, ty);
         __syncthreads();
         bool ok = true;
@@ -824,7 +831,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : kBulkMinBlocks<Q>)
             B::fill_nrm_carry(S, zs - 1, tid, gc);
             B::fill_nrm_carry(S, zs, tid, gc);
             __syncthreads();
-            typename B::Curv cv;
+            typename B::Curv cv(S, tid);
             cv.start(S, zs, tx, ty);
             __syncthreads();
             for (int z = zs; z < ze; ++z) {
