@@ -28,9 +28,8 @@
 
 namespace ssmd {
 
-// Resident work items per SM the register budget targets: 4 for D3Q19 (64
-// registers, its gradient carry in shared memory), 3 for D3Q27 (80 registers:
-// at 64 its 27 populations spill).
+// Resident work items per SM the register budget targets: 4 (64 registers),
+// with the long-lived gradient and curvature carries in shared memory.
 template <int Q>
 constexpr int kBulkMinBlocks = 4;
 
@@ -358,16 +357,13 @@ struct Bulk {
     // where S is the 1-4-1 sum and D the central difference along one axis.
     // Each plane's 3 x 3 neighbourhood is read once (9 loads, not 18 / 26).
     // The carried sums: plane p - 1: Gx, Gy, Sxy (D3Q27) / Ax, Ay, T (D3Q19);
-    // plane p: the same, and Cx, Cy (D3Q19).  D3Q27 keeps them in registers;
-    // D3Q19 keeps them in the thread's column of BulkSmem::carry, which frees
-    // the registers its 4-blocks-per-SM budget needs.
+    // plane p: the same, and Cx, Cy (D3Q19).  They live in the thread's column
+    // of BulkSmem::carry (rows 0-7), which frees the registers of the
+    // 4-blocks-per-SM budget.
     struct GradCarry {
-        float reg[8];
-        float *col; // BulkSmem::carry[0] + tid (D3Q19)
+        float *col; // &BulkSmem::carry[0][tid]
         __device__ __forceinline__ GradCarry(BulkSmem &S, int tid) : col(&S.carry[0][tid]) {}
-        __device__ __forceinline__ float &v(int k) {
-            return col[k * kThreads];
-        }
+        __device__ __forceinline__ float &v(int k) { return col[k * kThreads]; }
         __device__ __forceinline__ float &px() { return v(0); }
         __device__ __forceinline__ float &py() { return v(1); }
         __device__ __forceinline__ float &pz() { return v(2); }
@@ -492,7 +488,8 @@ struct Bulk {
     }
 
     // Per-thread curvature state along the column: C of the current plane and
-    // S - Z of the current and previous planes.
+    // S - Z of the current and previous planes, in rows 8-10 of the thread's
+    // column of BulkSmem::carry.
     struct Curv {
         float *col;
         __device__ __forceinline__ Curv(BulkSmem &S, int tid) : col(&S.carry[8][tid]) {}
