@@ -19,7 +19,7 @@ import os
 
 from . import _lib
 
-CANDIDATE_TILE_Z = (0, 8, 12, 16, 24, 32, 48, 64)
+CANDIDATE_TILE_Z = (0, 12, 14, 16, 20, 24, 28, 32, 48)
 
 
 def cache_path() -> str:
