@@ -84,6 +84,13 @@ struct Bulk {
     // phi^n at fluid cell (x, y, z) with linear index c, from the post-stream
     // phase populations (pull layout: direction q is read at c - c_q).
     static __device__ __forceinline__ float phi_from_g(const A &a, int x, int y, int z, uint32_t c) {
+        float g[7];
+        gather_g(a, x, y, z, c, g);
+        return (((((g[0] + g[1]) + g[2]) + g[3]) + g[4]) + g[5]) + g[6];
+    }
+
+    // The 7 post-stream phase populations of fluid cell (x, y, z), index c.
+    static __device__ __forceinline__ void gather_g(const A &a, int x, int y, int z, uint32_t c, float (&g)[7]) {
         const Geometry &G = a.geo;
         // 32-bit source cell indices (pull: direction q is read at c - c_q); a
         // fluid cell only wraps on an exact-periodic axis, selected per lane
@@ -95,14 +102,13 @@ struct Bulk {
         const uint32_t yp = c + (y == (int)G.ny - 1 ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx);
         const uint32_t zm = c + (z == 0 ? (uint32_t)(G.cells - G.nxy) : (uint32_t)-(int)G.nxy);
         const uint32_t zp = c + (z == (int)G.nz - 1 ? (uint32_t)-(int64_t)(G.cells - G.nxy) : G.nxy);
-        float s = Store<TG>::ld(a.gq_src[0] + c);
-        s += Store<TG>::ld(a.gq_src[1] + xm);
-        s += Store<TG>::ld(a.gq_src[2] + xp);
-        s += Store<TG>::ld(a.gq_src[3] + ym);
-        s += Store<TG>::ld(a.gq_src[4] + yp);
-        s += Store<TG>::ld(a.gq_src[5] + zm);
-        s += Store<TG>::ld(a.gq_src[6] + zp);
-        return s;
+        g[0] = Store<TG>::ld(a.gq_src[0] + c);
+        g[1] = Store<TG>::ld(a.gq_src[1] + xm);
+        g[2] = Store<TG>::ld(a.gq_src[2] + xp);
+        g[3] = Store<TG>::ld(a.gq_src[3] + ym);
+        g[4] = Store<TG>::ld(a.gq_src[4] + yp);
+        g[5] = Store<TG>::ld(a.gq_src[5] + zm);
+        g[6] = Store<TG>::ld(a.gq_src[6] + zp);
     }
 
     static __device__ __forceinline__ bool fluid(const Geometry &G, int x, int y, int z) {
@@ -137,33 +143,33 @@ struct Bulk {
         }
     }
 
-    // phi of ring element (hx, hy) = lattice cell (rx, ry) before wrapping,
-    // plane gz: fluid cells from g, ghost and outside cells 0 (the field
-    // computeForces sees, phaseField.cuh:118-142).
-    static __device__ __forceinline__ void phi_elem(const A &a, BulkSmem &S, int s, int hx, int hy, int rx, int ry,
-                                                    int gz, bool zfluid) {
-        const Geometry &G = a.geo;
-        const int gx = halo_axis(a, rx, G.nx, G.bcx == BC_PERIODIC);
-        const int gy = halo_axis(a, ry, G.ny, G.bcy == BC_PERIODIC);
-        float v = 0.f;
-        if (zfluid && gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi)
-            v = phi_from_g(a, gx, gy, gz, cell_index(G, gx, gy, gz));
-        S.phiZ[s][hy][hx] = v;
-    }
-
-    // Fill ring slot of plane pz with phi over the tile + 2-cell halo.
+    // Fill ring slot of plane pz with phi over the tile + 2-cell halo: fluid
+    // cells from g, ghost and outside cells 0 (the field computeForces sees,
+    // phaseField.cuh:118-142).  Both of a thread's elements gather before
+    // either sum, so their load latencies overlap.
     static __device__ void fill_phi(const A &a, BulkSmem &S, int x0, int y0, int pz, int tid) {
         const Geometry &G = a.geo;
+        const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC;
         const int gz = halo_axis(a, pz, G.nz, G.bcz == BC_PERIODIC);
         const int s = ringP(pz);
         const bool zfluid = gz >= G.z_lo && gz <= G.z_hi; // (gz = -1 outside a non-periodic axis)
+        auto fluid_xy = [&](int gx, int gy) { return gx >= G.x_lo && gx <= G.x_hi && gy >= G.y_lo && gy <= G.y_hi; };
         const int tx = tid % kTX, ty = tid / kTX;
-        phi_elem(a, S, s, tx + 2, ty + 2, x0 + tx, y0 + ty, gz, zfluid);
-        if (tid < kPhiBorder) {
-            int hx, hy;
+        const int ox = halo_axis(a, x0 + tx, G.nx, px), oy = halo_axis(a, y0 + ty, G.ny, py);
+        const bool fo = zfluid && fluid_xy(ox, oy);
+        const bool border = tid < kPhiBorder;
+        int hx = 0, hy = 0, bx = 0, by = 0;
+        if (border) {
             phi_border_pos(tid, hx, hy);
-            phi_elem(a, S, s, hx, hy, x0 - 2 + hx, y0 - 2 + hy, gz, zfluid);
+            bx = halo_axis(a, x0 - 2 + hx, G.nx, px);
+            by = halo_axis(a, y0 - 2 + hy, G.ny, py);
         }
+        const bool fb = border && zfluid && fluid_xy(bx, by);
+        float go[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, gb[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (fo) gather_g(a, ox, oy, gz, cell_index(G, ox, oy, gz), go);
+        if (fb) gather_g(a, bx, by, gz, cell_index(G, bx, by, gz), gb);
+        S.phiZ[s][ty + 2][tx + 2] = (((((go[0] + go[1]) + go[2]) + go[3]) + go[4]) + go[5]) + go[6];
+        if (border) S.phiZ[s][hy][hx] = (((((gb[0] + gb[1]) + gb[2]) + gb[3]) + gb[4]) + gb[5]) + gb[6];
     }
 
     static __device__ __forceinline__ float tofloat(float v) { return v; }
