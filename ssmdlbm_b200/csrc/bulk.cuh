@@ -251,8 +251,34 @@ struct Bulk {
         for (int z = zs; z < ze; ++z) {
             const float div = cv.advance(S, z, tx, ty);
             if (active) cell(a, S, x, y, z, tx, ty, div);
-            if (z + 2 <= ze) fill_nrm_carry(S, z + 2, tid, gc);
-            if (z + 4 <= ze + 1) fill_phi(a, S, x0, y0, z + 4, tid);
+            {
+                // fill_phi(z + 4) split around the normals of plane z + 2: the own
+                // column's 7 gathers are in flight while the normals are computed,
+                // then its sum and the border element (ghost / outside: 0)
+                const bool more = z + 4 <= ze + 1;
+                const int gz = halo_axis(a, z + 4, G.nz, G.bcz == BC_PERIODIC);
+                const bool zf = gz >= G.z_lo && gz <= G.z_hi;
+                const int ox = halo_axis(a, x, G.nx, G.bcx == BC_PERIODIC);
+                const int oy = halo_axis(a, y, G.ny, G.bcy == BC_PERIODIC);
+                float go[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (more && zf && ox >= G.x_lo && ox <= G.x_hi && oy >= G.y_lo && oy <= G.y_hi)
+                    gather_g(a, ox, oy, gz, cell_index(G, ox, oy, gz), go);
+                if (z + 2 <= ze) fill_nrm_carry(S, z + 2, tid, gc);
+                if (more) {
+                    const int sp = ringP(z + 4);
+                    S.phiZ[sp][ty + 2][tx + 2] = (((((go[0] + go[1]) + go[2]) + go[3]) + go[4]) + go[5]) + go[6];
+                    if (tid < kPhiBorder) {
+                        int hx, hy;
+                        phi_border_pos(tid, hx, hy);
+                        const int bx = halo_axis(a, x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
+                        const int by = halo_axis(a, y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
+                        float v = 0.f;
+                        if (zf && bx >= G.x_lo && bx <= G.x_hi && by >= G.y_lo && by <= G.y_hi)
+                            v = phi_from_g(a, bx, by, gz, cell_index(G, bx, by, gz));
+                        S.phiZ[sp][hy][hx] = v;
+                    }
+                }
+            }
             __syncthreads();
         }
     }
