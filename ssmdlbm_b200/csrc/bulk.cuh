@@ -249,8 +249,9 @@ struct Bulk {
         cv.start(S, zs, tx, ty);
         __syncthreads();
         for (int z = zs; z < ze; ++z) {
-            const float div = cv.advance(S, z, tx, ty);
-            if (active) cell(a, S, x, y, z, tx, ty, div);
+            // the plane terms after the population gathers are issued
+            if (active) cell_lazy(a, S, x, y, z, tx, ty, [&] { return cv.advance(S, z, tx, ty); });
+            else cv.advance(S, z, tx, ty);
             {
                 // fill_phi(z + 4) split around the normals of plane z + 2: the own
                 // column's 7 gathers are in flight while the normals are computed,
@@ -555,23 +556,27 @@ struct Bulk {
     static __device__ __forceinline__ void cell(const A &a, const BulkSmem &S, int x, int y, int z,
                                                 int tx, int ty, float div, const TF *fs = nullptr,
                                                 const TG *gs = nullptr) {
+        cell_lazy(a, S, x, y, z, tx, ty, [div] { return div; }, fs, gs);
+    }
+
+    // cell() with the normal divergence produced by divfn() after the
+    // population gathers are issued, so that their latency covers the plane
+    // terms (the gather loop passes Curv::advance).
+    template <class DivFn>
+    static __device__ __forceinline__ void cell_lazy(const A &a, const BulkSmem &S, int x, int y, int z, int tx,
+                                                     int ty, DivFn &&divfn, const TF *fs = nullptr,
+                                                     const TG *gs = nullptr) {
         const Geometry &G = a.geo;
         const Physics &P = a.phys;
         const bool px = G.bcx == BC_PERIODIC, py = G.bcy == BC_PERIODIC, pz = G.bcz == BC_PERIODIC;
         const uint32_t c0 = cell_index(G, x, y, z);
 
-        // ---- surface tension from the zeroed-ghost field (phaseField.cuh:246-293);
-        // div is the normal divergence of this cell, from the plane terms
+        // (the surface tension from the zeroed-ghost field, phaseField.cuh:246-293,
+        // follows the gathers below: its divergence comes from the plane terms)
         const int hx = tx + 2, hy = ty + 2; // phi ring centre
         const int nxh = tx + 1, nyh = ty + 1; // normal ring centre
         const int s0 = ringN(z);
         auto nat = [&](int comp) -> float { return S.nrm[s0][comp][nyh][nxh]; };
-        const float curvature = 3.0f * div;
-        const float sigma = a.clo_cs ? P.sigma * a.clo_cs[c0] : P.sigma;
-        const float stc = -sigma * curvature * nat(3);
-        const float fx = stc * nat(0);
-        const float fy = stc * nat(1);
-        const float fz = stc * nat(2);
 
         // ---- normals of the phase update from phi with ghost values (lbm.cu:157-224).
         // Away from ghost layers the raw and zeroed fields agree on the 3x3x3
@@ -660,6 +665,15 @@ struct Bulk {
                     });
             }
         }
+
+        // ---- surface tension: -sigma kappa |grad phi| n, kappa = 3 div
+        const float div = divfn();
+        const float curvature = 3.0f * div;
+        const float sigma = a.clo_cs ? P.sigma * a.clo_cs[c0] : P.sigma;
+        const float stc = -sigma * curvature * nat(3);
+        const float fx = stc * nat(0);
+        const float fy = stc * nat(1);
+        const float fz = stc * nat(2);
 
         // ---- hydrodynamics
         const Moments m = moments<Q>(f, fx, fy, fz);
