@@ -148,7 +148,7 @@ STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
 # DRAM bytes per cell of one bulk launch, dram__bytes_read.sum +
 # dram__bytes_write.sum from one ncu capture (profiles/, 128 x 128 x 256 case,
 # scaled to the lattice by its cell count)
-NCU_BYTES_PER_CELL = {(27, "f32"): 291.7}
+NCU_BYTES_PER_CELL = {(27, "f32"): 288.5}
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
