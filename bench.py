@@ -109,6 +109,8 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): NCCL
+    when CUDA is present, gloo otherwise (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -116,8 +118,10 @@ def dist_setup(n_gpus: int):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -126,9 +130,19 @@ def max_over_ranks(v: float, world: int) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_mlups(cells: int, steps: int, seconds: float, world: int) -> tuple:
+    """Whole-job MLUPS of `world` replicas of a lattice of `cells` cells, each
+    timed on its own device: the slowest replica's time (max over ranks) sets
+    the job time, every replica updated cells * steps.  Returns (seconds,
+    MLUPS)."""
+    t = max_over_ranks(seconds, world)
+    return t, cells * steps * world / t / 1e6
 
 
 def barrier(world: int):
@@ -152,7 +166,8 @@ NCU_BYTES_PER_CELL = {(27, "f32"): 288.5}
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
-    """Device time of `steps` steps replayed as 2-step graphs (max over ranks)."""
+    """Device time of `steps` steps replayed as 2-step graphs on this rank,
+    bracketed by barriers (replica_mlups takes the max over ranks)."""
     import torch
     sim.graph(2)
     sim.run_graph(max(1, warmup // 2), 2)
@@ -167,7 +182,7 @@ def time_graph(sim, steps: int, warmup: int, world: int):
     e1.synchronize()
     barrier(world)
     torch.cuda.synchronize()
-    return max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    return e0.elapsed_time(e1) / 1e3
 
 
 def bulk_launch_ms(sim, launches: int) -> float:
@@ -462,10 +477,9 @@ def run_ours(a, world, rank, local):
     tuned = autotune.tune(sim) if (a.path == 0 and not a.no_tune) else None
     sim.init()
     with ClockSampler(local) as clk:
-        dt = time_graph(sim, a.steps, a.warmup, world)
+        dt_local = time_graph(sim, a.steps, a.warmup, world)
     clocks = clk.summary()
-    mlups_rank = sim.cells * a.steps / dt / 1e6
-    value = mlups_rank * world
+    dt, value = replica_mlups(sim.cells, a.steps, dt_local, world)
     st = sim.reduce(raise_unstable=False)
 
     # live roofline of the dominant kernel
