@@ -56,56 +56,118 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 100 ms while active."""
+    """SM clocks, board power and clock-event (throttle) reasons sampled while
+    active: NVML read every 10 ms from a thread (the timed region of a default
+    run lasts a fraction of a second), `nvidia-smi -lms 100` when NVML cannot
+    be loaded.  Read-only: no clock or power setting is touched."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    PERIOD_S = 0.010
 
     def __init__(self, index: int):
-        self.index = index
+        self.index = index      # CUDA device ordinal of this rank
+        self.uuid = None        # the same device for NVML / nvidia-smi
+        try:
+            import torch
+            if torch.cuda.is_available():
+                self.uuid = "GPU-" + str(torch.cuda.get_device_properties(index).uuid)
+        except Exception:
+            self.uuid = None
         self.proc = None
+        self.thread = None
+        self.rows = []          # (sm_mhz, sm_max_mhz, power_w, set of reason names)
 
-    def __enter__(self):
+    # ---------------------------------------------------------------- NVML
+    def _nvml_start(self) -> bool:
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            try:
+                h = nv.nvmlDeviceGetHandleByUUID(self.uuid)
+            except Exception:
+                self.uuid = None
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        except Exception:
+            return False
+        self._nv, self._stop = nv, threading.Event()
+
+        def loop():
+            while True:
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((float(sm), float(smax), pw,
+                                      {n for n, b in bits.items() if r & b}))
+                except Exception:
+                    pass
+                if self._stop.wait(self.PERIOD_S):
+                    return
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+        return True
+
+    # ---------------------------------------------------------- nvidia-smi
+    def _smi_start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                ["nvidia-smi", "-i", self.uuid or str(self.index), f"--query-gpu={self.QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+
+    def _smi_stop(self):
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for l in out.splitlines():
+            c = [x.strip() for x in l.split(",")]
+            try:
+                row = (float(c[1]), float(c[2]), float(c[3]))
+            except (ValueError, IndexError):
+                continue
+            self.rows.append(row + ({n for n, v in zip(self.NAMES, c[5:9])
+                                     if v.lower().startswith("active")},))
+
+    def __enter__(self):
+        self.source = "nvml" if self._nvml_start() else "nvidia-smi"
+        if self.source == "nvidia-smi":
+            self._smi_start()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
             try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
+        elif self.proc is not None:
+            self._smi_stop()
 
     def summary(self):
-        if not getattr(self, "lines", None):
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm, smax, reasons, power = [], None, set(), []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            c = [x.strip() for x in l.split(",")]
-            try:
-                sm.append(float(c[1]))
-                smax = float(c[2])
-                power.append(float(c[3]))
-            except ValueError:
-                continue
-            for n, v in zip(names, c[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "power_w_max": max(power) if power else None, "samples": len(sm),
-                "reasons": sorted(reasons)}
+        sm = [r[0] for r in self.rows]
+        reasons = set().union(*(r[3] for r in self.rows))
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm), "sm_max_mhz": self.rows[-1][1],
+                "power_w_max": round(max(r[2] for r in self.rows), 1), "samples": len(sm),
+                "source": self.source, "reasons": sorted(reasons)}
 
 
 def dist_setup(n_gpus: int):

@@ -25,7 +25,9 @@ bench.barrier(world)
 import torch.distributed as dist
 assert dist.get_backend() == "gloo"
 dist.destroy_process_group()
-print(json.dumps({{"rank": rank, "t": t, "mlups": mlups}}))
+# one file per rank: two ranks printing to one pipe can interleave their lines
+with open(os.path.join({out!r}, f"rank{{rank}}.json"), "w") as f:
+    json.dump({{"rank": rank, "t": t, "mlups": mlups}}, f)
 '''
 
 
@@ -38,13 +40,13 @@ def _free_port() -> int:
 @pytest.mark.timeout(300)
 def test_replica_mlups_takes_the_slowest_rank(tmp_path):
     script = tmp_path / "rank.py"
-    script.write_text(RANK_SCRIPT.format(root=ROOT))
+    script.write_text(RANK_SCRIPT.format(root=ROOT, out=str(tmp_path)))
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="", MASTER_ADDR="127.0.0.1")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr=127.0.0.1", f"--master-port={_free_port()}", str(script)]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=240, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
-    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    lines = [json.loads((tmp_path / f"rank{k}.json").read_text()) for k in range(2)]
     assert sorted(d["rank"] for d in lines) == [0, 1]
     for d in lines:
         assert d["t"] == 2.0  # the slower replica sets the job time
@@ -55,3 +57,30 @@ def test_single_process_needs_no_process_group():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.replica_mlups(1000, 10, 0.5, 1) == (0.5, 1000 * 10 / 0.5 / 1e6)
+
+
+def test_clock_summary_reads_nvidia_smi_rows():
+    """The sampler's fallback parses `nvidia-smi --format=csv,noheader,nounits`
+    rows and reports the median SM clock and every throttle reason seen."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class FakeProc:
+        def terminate(self):
+            pass
+
+        def communicate(self, timeout=None):
+            rows = ["0, 1965, 1965, 390.5, 0x0, Not Active, Not Active, Not Active, Not Active",
+                    "0, 1800, 1965, 998.0, 0x4, Not Active, Not Active, Not Active, Active",
+                    "0, 1965, 1965, 401.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+                    "0, [N/A], 1965, 1.0, 0x0, Not Active, Not Active, Not Active, Not Active"]
+            return "\n".join(rows) + "\n", ""
+
+    c = bench.ClockSampler(0)
+    c.source, c.proc = "nvidia-smi", FakeProc()
+    c.__exit__(None, None, None)
+    s = c.summary()
+    assert s["samples"] == 3 and s["sm_mhz"] == 1965.0 and s["sm_min_mhz"] == 1800.0
+    assert s["sm_max_mhz"] == 1965.0 and s["power_w_max"] == 998.0
+    assert s["reasons"] == ["sw_power_cap"]
+    assert bench.ClockSampler(0).summary()["reasons"] == ["unsampled"]
