@@ -188,8 +188,11 @@ inline void bulk_slots(int &per_sm, int &sms) {
 // chunks), each holding a resident slot for its planes plus kProloguePlanes
 // (the ring prologue), the next item starting on the first slot to free.  On
 // B200 this model tracks the measured kernel time across chunk sizes
-// (correlation 0.98 on the 128 x 128 x 512 jet, chunks of 12-32 planes).
+// (correlation 0.98 on the 128 x 128 x 512 jet, chunks of 12-32 planes, and
+// it ranks 56 planes, one wave of 4 items per SM, first among 28-64 there,
+// as measured).
 constexpr double kProloguePlanes = 4.0;
+constexpr int kMaxAutoChunk = 64;
 
 inline double chunk_makespan(long cols, int nzf, int zc, int slots) {
     std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
@@ -208,7 +211,7 @@ inline double chunk_makespan(long cols, int nzf, int zc, int slots) {
 }
 
 // Bulk tiling: 32 x 8 columns.  Unless the caller fixes tile_z, the z chunk
-// (8..32 planes, the range the model was checked on) minimises
+// (8..64 planes, the range the model was checked on) minimises
 // chunk_makespan; the choice is cached per lattice shape and slot count (the
 // search costs a few ms on the largest lattices).
 inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tiles_x, int &tiles_y,
@@ -225,7 +228,7 @@ inline void tiling(const ssmd_params &p, const Geometry &G, int slots, int &tile
         if (cols != c_cols || nzf != c_nzf || slots != c_slots) {
             double best = 1e300;
             int arg = std::min(16, nzf);
-            for (int zc = std::min(8, nzf); zc <= std::min(nzf, 32); ++zc) {
+            for (int zc = std::min(8, nzf); zc <= std::min(nzf, kMaxAutoChunk); ++zc) {
                 const double t = chunk_makespan(cols, nzf, zc, slots);
                 if (t <= best * (1.0 + 1e-9)) { // ties: the longer chunk (fewer prologues)
                     best = std::min(best, t);
