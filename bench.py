@@ -221,10 +221,10 @@ def workload(storage: int, q: int = Q):
 
 STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
 
-# DRAM bytes per cell of one bulk launch, dram__bytes_read.sum +
-# dram__bytes_write.sum from one ncu capture (profiles/, 128 x 128 x 256 case,
-# scaled to the lattice by its cell count)
-NCU_BYTES_PER_CELL = {(27, "f32"): 288.5}
+# DRAM bytes per cell of one bulk launch on the 128 x 128 x 512 jet,
+# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of that
+# launch (profiles/), keyed by (velocity set, storage)
+NCU_BYTES_PER_CELL = {(27, "f32"): 294.0, (19, "f32"): 228.4, (27, "f16"): 136.6}
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
@@ -599,7 +599,7 @@ def run_ours(a, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": (int(NCU_BYTES_PER_CELL[(a.vs, a.storage)] * NX * NY * NZ)
-                                 if (a.vs, a.storage) in NCU_BYTES_PER_CELL else None),
+                                 if (a.vs, a.storage) in NCU_BYTES_PER_CELL and not a.size else None),
                      "peak_kind": peak_kind, "kernel": f"ssmd::bulk_kernel<{a.vs},{a.storage}>",
                      "bytes_per_cell": b_alg(a.vs, s_f0), "launch_ms": round(bulk_ms, 4)},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
