@@ -510,8 +510,9 @@ def run_production(net, steps: int = 200, update_every: int = 10):
 
 def run_closure(full: bool):
     """Coarse-plus-closure run against the fine run it learns from (D3Q19 oil
-    jet, 2x coarsening).  Default: fine 128 x 128 x 512 for 4000 steps;
-    --closure-full: fine 256 x 256 x 1024 for 20000 steps (one seed)."""
+    jet, 2x coarsening).  Default (full): fine 256 x 256 x 1024 for 20000
+    steps, the size of the closure study's fine runs (one seed of its eight);
+    --closure-small: fine 128 x 128 x 512 for 4000 steps."""
     from ssmdlbm_b200 import closure, configs
     if full:
         shape, steps, every, spin, train, diam = (256, 256, 1024), 20000, 1000, 10000, 4000, 32
@@ -566,8 +567,12 @@ def run_ours(a, world, rank, local):
     del sim
     torch.cuda.empty_cache()
 
+    # the single-GPU legs below (storage / velocity-set variants, sweep,
+    # closure, precision, production) run at N = 1 only: they are one-GPU
+    # measurements, and under torchrun they would only hold the other GPUs
+    extras = world == 1 and not a.quick
     variants = {}
-    if not a.quick:
+    if extras:
         for name, q, stg in (("d3q27_f16", 27, _lib.STORAGE_F16), ("d3q27_bf16", 27, _lib.STORAGE_BF16),
                              ("d3q19_f32", 19, _lib.STORAGE_F32), ("d3q19_f16", 19, _lib.STORAGE_F16)):
             pv = workload(stg, q)
@@ -585,14 +590,18 @@ def run_ours(a, world, rank, local):
             del sv
             torch.cuda.empty_cache()
 
-    sweep = run_sweep() if not a.quick else None
-    closure_line, net = run_closure(a.closure_full) if (not a.quick and not a.no_closure) else (None, None)
-    precision = run_precision() if not a.quick else None
-    production = run_production(net) if (not a.quick and not a.no_production) else None
+    sweep = run_sweep() if extras else None
+    closure_line, net = run_closure(not a.closure_small) if (extras and not a.no_closure) else (None, None)
+    precision = run_precision() if extras else None
+    production = run_production(net) if (extras and not a.no_production) else None
 
     p.bulk_path, p.tile_z = sim_path, sim_tz
-    e2e_mlups, h2d, d2h = e2e_run(p, max(20, min(a.steps, 200)))
-    e2e_mlups = e2e_mlups * world
+    e2e_steps = max(20, min(a.steps, 200))
+    barrier(world)
+    e2e_local, h2d, d2h = e2e_run(p, e2e_steps)
+    # every replica ran the same job: the slowest one sets the time
+    e2e_t = max_over_ranks(p.nx * p.ny * p.nz * e2e_steps / (e2e_local * 1e6), world)
+    e2e_mlups = world * p.nx * p.ny * p.nz * e2e_steps / e2e_t / 1e6
 
     line = {
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
@@ -666,7 +675,8 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--quick", action="store_true", help="skip the storage / velocity-set variants")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline only: skip the variants, sweep, closure, precision and production legs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", default=None, help="nx,ny,nz of a smaller lattice (profiling runs)")
     ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
@@ -675,8 +685,8 @@ def main() -> int:
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     ap.add_argument("--no-production", action="store_true",
                     help="skip the 384 x 384 x 1536 production-lattice leg")
-    ap.add_argument("--closure-full", action="store_true",
-                    help="closure leg at 256 x 256 x 1024, 20000 steps (minutes)")
+    ap.add_argument("--closure-small", action="store_true",
+                    help="closure leg at 128 x 128 x 512, 4000 steps (seconds) instead of 256 x 256 x 1024, 20000 steps")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                     help="bulk kernel path: 0 auto, 1 gathers, 2 TMA phi boxes, 3 TMA population slabs")
     a = ap.parse_args()

@@ -9,11 +9,17 @@ the library's kernels.
 Lattice units follow acoustic scaling: the coarse lattice has twice the
 spacing and twice the time step, so velocities are unchanged, viscosity and
 mobility halve (nu dt / dx^2), surface tension halves (sigma dt^2 / dx^3),
-the nozzle radius halves, and one coarse step spans two fine steps.
+the nozzle radius halves, and one coarse step spans two fine steps.  The
+interface keeps its physical thickness, so its width in cells halves too (4
+fine cells, 2 coarse), and the sharpening rate gamma = 4 M / (W c_s^2), with
+both M and W halved, keeps its lattice value.  (Keeping 4 cells instead
+doubles the physical thickness: on the 128 x 128 x 512 jet the plain coarse
+run then loses 12.7 % of the fine run's phi volume instead of 6.8 %.)
 """
 from __future__ import annotations
 
 import ctypes
+import math
 import time
 from dataclasses import dataclass, field
 
@@ -58,7 +64,7 @@ def coarse_params(p: Params) -> Params:
         setattr(q, omco_name, f32(1) - f32(1.0 / (0.5 + 3.0 * float(nu))))
     q.omco_ref = q.omco_water
     q.sigma = f32(p.sigma) * f32(0.5)
-    q.gamma = f32(p.gamma) * f32(0.5)  # mobility halves, width stays 4 cells
+    q.gamma = f32(p.gamma)  # mobility and width (in cells) both halve
     mob = (1.0 / float(p.omega_g) - 0.5) * CS2_PHASE * 0.5
     q.omega_g = f32(1.0 / (0.5 + mob / CS2_PHASE))
     q.oil_cx = f32((q.nx - 1) * 0.5) if abs(p.oil_cx - (p.nx - 1) * 0.5) < 1e-3 else f32(p.oil_cx * 0.5)
@@ -176,8 +182,26 @@ def _view(coarse: torch.Tensor, nc: int) -> LBMFields:
     return f
 
 
-def _stats_snapshot(sim, acc: dict) -> None:
-    uz, phi = sim.centreline()
+def _coarse_axis_cells(c: float) -> list:
+    """Coarse cells whose mean is the centreline at coarse coordinate c."""
+    return sorted({int(math.floor(c)), int(math.ceil(c))})
+
+
+def _stats_snapshot(sim, acc: dict, cp: Params | None = None) -> None:
+    """Accumulate the centreline profiles.  On the fine lattice (cp = the
+    coarse lattice's parameters) the profile is the fine field filtered onto
+    the coarse cells the coarse run samples: fine cells 2i and 2i + 1 under
+    coarse cell i, so both runs average over the same region around the axis
+    (the fine lattice's own nearest cells sit half as far from it)."""
+    if cp is None:
+        uz, phi = sim.centreline()
+    else:
+        uz = phi = 0.0
+        cells = [(i, j) for i in _coarse_axis_cells(float(cp.oil_cx)) for j in _coarse_axis_cells(float(cp.oil_cy))]
+        for i, j in cells:
+            u, f = sim.centreline(2 * i + 0.5, 2 * j + 0.5)
+            uz, phi = uz + u, phi + f
+        uz, phi = uz / len(cells), phi / len(cells)
     acc["uz"] = acc.get("uz", 0) + uz
     acc["phi"] = acc.get("phi", 0) + phi
     acc["n"] = acc.get("n", 0) + 1
@@ -221,7 +245,7 @@ def fine_run(p: Params, steps: int, sample_every: int, spinup: int, nut_max: flo
         t_dev += _timed_steps(sim, k)
         done += k
         if done >= spinup:
-            _stats_snapshot(sim, acc)
+            _stats_snapshot(sim, acc, cp)
             if data is not None:
                 st = sim.stream
                 check(L.ssmd_closure_filter(ctypes.byref(sim.p), ctypes.byref(sim.fields), coarse.data_ptr(),

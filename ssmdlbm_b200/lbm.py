@@ -172,13 +172,19 @@ class Simulation:
                                     ctypes.byref(a), ctypes.byref(b), self.stream))
         return a.value, b.value
 
-    def centreline(self):
-        """Mean u_z and phi along the oil-nozzle axis, per z (FP64 numpy arrays).
-        Needs the macroscopic fields of a step with store_macros."""
+    def centreline(self, cx: float | None = None, cy: float | None = None):
+        """Mean u_z and phi along the oil-nozzle axis, per z (FP64 numpy arrays):
+        over the one, two or four cells nearest (cx, cy), by default the nozzle
+        centre.  Needs the macroscopic fields of a step with store_macros."""
+        p = self.p
+        if cx is not None or cy is not None:
+            p = self.p.copy()
+            p.oil_cx = self.p.oil_cx if cx is None else cx
+            p.oil_cy = self.p.oil_cy if cy is None else cy
         uz = torch.zeros(int(self.p.nz), dtype=torch.float64, device=self.device)
         phi = torch.zeros_like(uz)
         torch.cuda.synchronize(self.device)
-        check(lib().ssmd_centreline(ctypes.byref(self.p), ctypes.byref(self.fields), uz.data_ptr(),
+        check(lib().ssmd_centreline(ctypes.byref(p), ctypes.byref(self.fields), uz.data_ptr(),
                                     phi.data_ptr(), self.stream))
         self.sync()
         return uz.cpu().numpy(), phi.cpu().numpy()

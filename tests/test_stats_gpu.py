@@ -66,6 +66,25 @@ def test_centreline_matches_oracle_after_jet_steps():
     assert uz[1] > 0.04  # the jet leaves the nozzle along the axis
 
 
+def test_centreline_off_axis_is_the_block_mean():
+    """centreline(cx, cy) averages the cells nearest (cx, cy); the fine-run
+    statistics of the closure experiment use it to filter the fine field onto
+    the coarse cells around the axis."""
+    from ssmdlbm_b200.closure import _coarse_axis_cells
+    p = configs.oil_jet(32, 32, 64, 19, tau=0.56, diam=8, noise=0.01, seed=2)
+    sim = _sim(p)
+    sim.init()
+    sim.step(20, store_macros=True)
+    uzf = sim.field("uz").astype(np.float64)
+    phif = sim.field("phi").astype(np.float64)
+    uz, phi = sim.centreline(12.5, 20.5)
+    assert np.allclose(uz, uzf[:, 20:22, 12:14].mean(axis=(1, 2)), rtol=1e-12, atol=1e-15)
+    assert np.allclose(phi, phif[:, 20:22, 12:14].mean(axis=(1, 2)), rtol=1e-12, atol=1e-15)
+    uz, _ = sim.centreline(7.0, 9.0)  # a single column
+    assert np.allclose(uz, uzf[:, 9, 7], rtol=1e-12, atol=1e-15)
+    assert _coarse_axis_cells(15.5) == [15, 16] and _coarse_axis_cells(15.0) == [15]
+
+
 def test_checkpoint_resume_is_bit_exact(tmp_path):
     p = configs.oil_jet(32, 24, 40, 19, tau=0.56, diam=6, noise=0.01, seed=4)
     a = _sim(p)
