@@ -19,7 +19,8 @@ import os
 
 from . import _lib
 
-CANDIDATE_TILE_Z = (0, 12, 14, 16, 20, 24, 28, 32, 48)
+# 0: the library's own choice (a makespan model of the block scheduling, 8-64 planes)
+CANDIDATE_TILE_Z = (0, 12, 16, 20, 24, 28, 32, 48, 56, 64)
 
 
 def cache_path() -> str:
