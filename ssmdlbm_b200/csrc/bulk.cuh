@@ -98,19 +98,21 @@ struct Bulk {
         // fluid cell only wraps on an exact-periodic axis, selected per lane
         // (no branch, so a warp never runs two paths).  Population q of cell i
         // is then one wide multiply-add away from the warp-uniform base g + q N.
+        // The loads keep their lines in L2 (evict-last): the neighbouring
+        // tiles' ring borders and this cell's own update read them again.
         const uint32_t xm = c + (x == 0 ? G.nx - 1 : (uint32_t)-1);
         const uint32_t xp = c + (x == (int)G.nx - 1 ? (uint32_t)(1 - (int)G.nx) : 1u);
         const uint32_t ym = c + (y == 0 ? G.nxy - G.nx : (uint32_t)-(int)G.nx);
         const uint32_t yp = c + (y == (int)G.ny - 1 ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx);
         const uint32_t zm = c + (z == 0 ? (uint32_t)(G.cells - G.nxy) : (uint32_t)-(int)G.nxy);
         const uint32_t zp = c + (z == (int)G.nz - 1 ? (uint32_t)-(int64_t)(G.cells - G.nxy) : G.nxy);
-        g[0] = Store<TG>::ld(a.gq_src[0] + c);
-        g[1] = Store<TG>::ld(a.gq_src[1] + xm);
-        g[2] = Store<TG>::ld(a.gq_src[2] + xp);
-        g[3] = Store<TG>::ld(a.gq_src[3] + ym);
-        g[4] = Store<TG>::ld(a.gq_src[4] + yp);
-        g[5] = Store<TG>::ld(a.gq_src[5] + zm);
-        g[6] = Store<TG>::ld(a.gq_src[6] + zp);
+        g[0] = Store<TG>::ld_keep(a.gq_src[0] + c);
+        g[1] = Store<TG>::ld_keep(a.gq_src[1] + xm);
+        g[2] = Store<TG>::ld_keep(a.gq_src[2] + xp);
+        g[3] = Store<TG>::ld_keep(a.gq_src[3] + ym);
+        g[4] = Store<TG>::ld_keep(a.gq_src[4] + yp);
+        g[5] = Store<TG>::ld_keep(a.gq_src[5] + zm);
+        g[6] = Store<TG>::ld_keep(a.gq_src[6] + zp);
     }
 
     static __device__ __forceinline__ bool fluid(const Geometry &G, int x, int y, int z) {

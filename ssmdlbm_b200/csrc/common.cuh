@@ -13,6 +13,19 @@ namespace ssmd {
 // ------------------------------------------------------------- storage
 // Populations are kept "shifted" (f - w_q, reference src/cuda/utils.cuh:67-99);
 // the reduced types only change the element type, arithmetic stays FP32.
+// L2 policy for loads whose lines are read again within a few planes: the
+// phase populations gathered into the phi ring are gathered again by the
+// neighbouring tiles' ring borders and by the cell update four planes later,
+// while the hydrodynamic stream passing through L2 in between is touched
+// once.  Marking the ring's loads evict-last keeps more of those lines (on
+// the 128 x 128 x 512 jet: D3Q27 FP32 0.483 -> 0.474 ms, D3Q19 FP32 0.397 ->
+// 0.391 ms).  (createpolicy / ld.global.nc.L2::cache_hint, sm_80 and later.)
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 template <class T>
 struct Store;
 
@@ -20,12 +33,22 @@ template <>
 struct Store<float> {
     static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
     static __device__ __forceinline__ float ldc(const float *p) { return *p; } // coherent (same-kernel writers)
+    static __device__ __forceinline__ float ld_keep(const float *p) { // read-only, L2 evict-last
+        float v;
+        asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_keep_policy()));
+        return v;
+    }
     static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
 };
 template <>
 struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
     static __device__ __forceinline__ float ldc(const __half *p) { return __half2float(*p); }
+    static __device__ __forceinline__ float ld_keep(const __half *p) {
+        unsigned short v;
+        asm("ld.global.nc.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(l2_keep_policy()));
+        return __half2float(__ushort_as_half(v));
+    }
     static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v); }
 };
 template <>
@@ -34,6 +57,11 @@ struct Store<__nv_bfloat16> {
         return __bfloat162float(__ldg(p));
     }
     static __device__ __forceinline__ float ldc(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ float ld_keep(const __nv_bfloat16 *p) {
+        unsigned short v;
+        asm("ld.global.nc.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(l2_keep_policy()));
+        return __bfloat162float(__ushort_as_bfloat16(v));
+    }
     static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
