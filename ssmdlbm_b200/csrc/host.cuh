@@ -308,10 +308,17 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     auto grid2 = [&](uint32_t n0, uint32_t n1) {
         return dim3((n0 + b2.x - 1) / b2.x, (n1 + b2.y - 1) / b2.y);
     };
-    if (G.bcy == BC_JET) bc_water_inflow<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
-    if (G.bcz == BC_JET) bc_oil_inflow<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
-    if (G.bcy == BC_JET) bc_outflow_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
-    if (G.bcz == BC_JET) bc_outflow_z<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+    if (G.bcz == BC_JET && G.bcy != BC_JET && G.nz >= 3) {
+        // the two z faces are independent: one launch (reference order otherwise)
+        dim3 g = grid2(G.nx, G.ny);
+        g.z = 2;
+        bc_jet_z<Q, T, T><<<g, b2, 0, st>>>(a);
+    } else {
+        if (G.bcy == BC_JET) bc_water_inflow<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+        if (G.bcz == BC_JET) bc_oil_inflow<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+        if (G.bcy == BC_JET) bc_outflow_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+        if (G.bcz == BC_JET) bc_outflow_z<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+    }
     if (G.bcx == BC_COPY) bc_copy_x<Q, T, T><<<grid2(G.ny, G.nz), b2, 0, st>>>(a);
     if (G.bcy == BC_COPY) bc_copy_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
     if (flags & SSMD_STEP_AVERAGE) {

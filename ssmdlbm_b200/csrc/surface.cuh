@@ -276,6 +276,16 @@ template <int Q, class TF, class TG>
 __global__ void bc_outflow_z(const StepArgs<TF, TG> a) {
     bc_outflow_z_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
 }
+// Oil inflow (blockIdx.z 0) and outflow z (blockIdx.z 1) in one launch, for a
+// lattice whose only jet faces are the z pair: inflow writes plane 0 and reads
+// plane 1, outflow writes plane nz-1 and reads plane nz-2, so with nz >= 3
+// neither reads what the other writes and their order does not matter.
+template <int Q, class TF, class TG>
+__global__ void bc_jet_z(const StepArgs<TF, TG> a) {
+    const int i0 = (int)(threadIdx.x + blockIdx.x * blockDim.x), i1 = (int)(threadIdx.y + blockIdx.y * blockDim.y);
+    if (blockIdx.z == 0) bc_oil_inflow_at<Q>(a, i0, i1);
+    else bc_outflow_z_at<Q>(a, i0, i1);
+}
 template <int Q, class TF, class TG>
 __global__ void bc_copy_x(const StepArgs<TF, TG> a) {
     bc_copy_x_at<Q>(a, (int)(threadIdx.x + blockIdx.x * blockDim.x), (int)(threadIdx.y + blockIdx.y * blockDim.y));
