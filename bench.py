@@ -340,13 +340,14 @@ def cpu_baseline(p, steps: int = 3):
 def run_sweep(steps: int = 40):
     """The 48-lattice sweep (N x N x 4N, N in {32, 48, 64, 96}, seed 2; D3Q19
     f32): batched persistent launches replayed as graphs, z-chunk height
-    tuned over {8, 16, 32}, against the same steps issued lattice by lattice."""
+    tuned over {8, 16, 32, 48, 64}, against the same steps issued lattice by
+    lattice."""
     import torch
     from ssmdlbm_b200.batch import Sweep, sweep_params
     sw = Sweep(sweep_params(48, seed=2))
     sw.init()
     best = None
-    for tz in (8, 16, 32):
+    for tz in (8, 16, 32, 48, 64):
         sw.set_tile_z(tz)
         sw.timed(4)
         dt = sw.timed(steps)
