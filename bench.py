@@ -224,7 +224,7 @@ STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
 # DRAM bytes per cell of one bulk launch on the 128 x 128 x 512 jet,
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of that
 # launch (profiles/), keyed by (velocity set, storage)
-NCU_BYTES_PER_CELL = {(27, "f32"): 278.5, (19, "f32"): 214.4, (27, "f16"): 136.6}
+NCU_BYTES_PER_CELL = {(27, "f32"): 278.5, (19, "f32"): 214.4, (27, "f16"): 133.7}
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
