@@ -63,7 +63,9 @@ typedef struct CUgraphExec_st *ssmd_graph_exec_t;
 /* ------------------------------------------------------- storage types */
 #define SSMD_STORAGE_F32 0  /* f - w_q and g as float                        */
 #define SSMD_STORAGE_F16 1  /* f - w_q and g as IEEE half (round to nearest) */
-#define SSMD_STORAGE_BF16 2 /* f - w_q and g as bfloat16 (round to nearest)  */
+#define SSMD_STORAGE_BF16 2 /* f - w_q as bfloat16, g as IEEE half (both round
+                               to nearest; g carries phi in [0, 1], which
+                               needs mantissa bits rather than range)     */
 
 /* ------------------------------------------------- bulk kernel variants */
 #define SSMD_PATH_AUTO 0   /* library choice (currently SSMD_PATH_GATHER)        */

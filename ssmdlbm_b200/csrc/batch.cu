@@ -65,15 +65,15 @@ int prepare(const ssmd_params *params, const LBMFields *fields, int32_t count, v
         const ssmd_params &p = params[i];
         const LBMFields &fl = fields[i];
         for (int par = 0; par < 2; ++par) {
-            StepArgs<T, T> &a = inst[i].args[par];
+            StepArgs<T, phase_t<T>> &a = inst[i].args[par];
             a.geo = make_geometry(p);
             a.phys = make_physics(p);
             a.fld = make_fields(fl);
             const bool even = par == 0;
             a.f_src = static_cast<const T *>(even ? fl.f : p.f_alt);
             a.f_dst = static_cast<T *>(even ? p.f_alt : fl.f);
-            a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
-            a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
+            a.g_src = static_cast<const phase_t<T> *>(even ? fl.g : p.g_alt);
+            a.g_dst = static_cast<phase_t<T> *>(even ? p.g_alt : fl.g);
             set_bases(a, Q);
             a.status = status_of(p);
             set_closure(a, p);

@@ -27,7 +27,7 @@ struct BatchHeader {
 
 template <class T>
 struct BatchInst {
-    StepArgs<T, T> args[2]; // parity 0: A -> B, parity 1: B -> A
+    StepArgs<T, phase_t<T>> args[2]; // parity 0: A -> B, parity 1: B -> A
     uint32_t item_begin;
     uint32_t items;
     uint32_t pad[2];
@@ -36,9 +36,9 @@ struct BatchInst {
 template <int Q, class T>
 __global__ void __launch_bounds__(kThreads, kBulkMinBlocks<Q>)
     bulk_batch_kernel(BatchHeader *hdr, const BatchInst<T> *inst, int parity, uint32_t flags) {
-    using B = Bulk<Q, T, T>;
+    using B = Bulk<Q, T, phase_t<T>>;
     __shared__ BulkSmem S;
-    __shared__ StepArgs<T, T> sa;
+    __shared__ StepArgs<T, phase_t<T>> sa;
     __shared__ uint32_t s_item, s_inst;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kTX * ty;
     const uint32_t count = hdr->count, total = hdr->total_items;
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kThreads, kBulkMinBlocks<Q>)
         {   // this instance's arguments into shared memory
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&inst[s_inst].args[parity]);
             uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
-            for (int k = tid; k < (int)(sizeof(StepArgs<T, T>) / 4); k += kThreads) dst[k] = src[k];
+            for (int k = tid; k < (int)(sizeof(StepArgs<T, phase_t<T>>) / 4); k += kThreads) dst[k] = src[k];
         }
         __syncthreads();
         if (tid == 0) sa.flags = flags;
@@ -95,7 +95,7 @@ enum : int { BK_WATER_IN = 0, BK_OIL_IN, BK_OUT_Y, BK_OUT_Z, BK_COPY_X, BK_COPY_
 
 template <int Q, class T, int K>
 __global__ void bc_batch_kernel(const BatchInst<T> *inst, int parity) {
-    const StepArgs<T, T> &a = inst[blockIdx.z].args[parity];
+    const StepArgs<T, phase_t<T>> &a = inst[blockIdx.z].args[parity];
     const int i0 = threadIdx.x + blockIdx.x * blockDim.x, i1 = threadIdx.y + blockIdx.y * blockDim.y;
     const Geometry &G = a.geo;
     if constexpr (K == BK_WATER_IN) { if (G.bcy == BC_JET) bc_water_inflow_at<Q>(a, i0, i1); }

@@ -771,6 +771,7 @@ __global__ void __launch_bounds__(kThreads, PATH == 3 ? 2 : kBulkMinBlocks<Q>)
     if constexpr (PATH == 3) {
         extern __shared__ __align__(128) unsigned char dyn3[];
         using SL = Slab<TF>;
+        static_assert(sizeof(TF) == sizeof(TG), "a slab stage holds f and g slabs of one element size");
         constexpr size_t STAGE = (size_t)(Q + 7) * SL::BYTES;
         auto fstage = [&](int k) { return reinterpret_cast<TF *>(dyn3 + (k & 1) * STAGE); };
         auto gstage = [&](int k) { return reinterpret_cast<TG *>(dyn3 + (k & 1) * STAGE + (size_t)Q * SL::BYTES); };

@@ -155,7 +155,7 @@ static __global__ void advance_avg_kernel(DeviceStatus *status) { status->avg_t 
 // Dynamic shared memory of a bulk instantiation (TMA boxes or slabs).
 template <int Q, class T, int PATH>
 constexpr size_t bulk_dyn_smem() {
-    return PATH == 2 ? GBox<T>::SMEM : (PATH == 3 ? Slab<T>::template smem<Q>() : 0);
+    return PATH == 2 ? GBox<phase_t<T>>::SMEM : (PATH == 3 ? Slab<T>::template smem<Q>() : 0);
 }
 
 // Resident bulk work items per SM for this instantiation (queried once per
@@ -170,8 +170,9 @@ inline void bulk_slots(int &per_sm, int &sms) {
         int n = 0, m = 0;
         const size_t dyn = bulk_dyn_smem<Q, T, PATH>();
         if (dyn > 0)
-            cudaFuncSetAttribute(bulk_kernel<Q, T, T, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bulk_kernel<Q, T, T, PATH>, kThreads, dyn) !=
+            cudaFuncSetAttribute(bulk_kernel<Q, T, phase_t<T>, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dyn);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bulk_kernel<Q, T, phase_t<T>, PATH>, kThreads, dyn) !=
             cudaSuccess)
             n = 1;
         if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) m = 148;
@@ -256,15 +257,16 @@ inline void set_closure(StepArgs<TF, TG> &a, const ssmd_params &p) {
 template <int Q, class T>
 int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32_t flags,
                 cudaStream_t st) {
-    StepArgs<T, T> a{};
+    using TG = phase_t<T>;
+    StepArgs<T, TG> a{};
     a.geo = make_geometry(p);
     a.phys = make_physics(p);
     a.fld = make_fields(fl);
     const bool even = (step & 1ull) == 0ull;
     a.f_src = static_cast<const T *>(even ? fl.f : p.f_alt);
     a.f_dst = static_cast<T *>(even ? p.f_alt : fl.f);
-    a.g_src = static_cast<const T *>(even ? fl.g : p.g_alt);
-    a.g_dst = static_cast<T *>(even ? p.g_alt : fl.g);
+    a.g_src = static_cast<const TG *>(even ? fl.g : p.g_alt);
+    a.g_dst = static_cast<TG *>(even ? p.g_alt : fl.g);
     set_bases(a, Q);
     a.status = status_of(p);
     set_closure(a, p);
@@ -274,10 +276,10 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     CUtensorMap gmap{}, fmap{};
     int path = p.bulk_path == SSMD_PATH_AUTO ? SSMD_PATH_GATHER : p.bulk_path;
     if (path == SSMD_PATH_TMA &&
-        !encode_populations<T>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, GBox<T>::WX, kHY))
+        !encode_populations<TG>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, GBox<TG>::WX, kHY))
         return fail(SSMD_ERR_UNSUPPORTED, "TMA path needs nx * element size to be a multiple of 16 bytes");
     if (path == SSMD_PATH_SLAB &&
-        !(encode_populations<T>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, Slab<T>::WX, kTY) &&
+        !(encode_populations<TG>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, Slab<TG>::WX, kTY) &&
           encode_populations<T>(&fmap, a.f_src, a.geo.nx, a.geo.ny, a.geo.nz, Q, Slab<T>::WX, kTY)))
         return fail(SSMD_ERR_UNSUPPORTED, "slab path needs nx * element size to be a multiple of 16 bytes");
     int per_sm = 1, sms = 1;
@@ -295,11 +297,11 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     profile_next(&ev0, &ev1);
     if (ev0) cudaEventRecord(ev0, st);
     if (path == SSMD_PATH_TMA)
-        bulk_kernel<Q, T, T, 2><<<nblk, blk, bulk_dyn_smem<Q, T, 2>(), st>>>(a, gmap, fmap);
+        bulk_kernel<Q, T, TG, 2><<<nblk, blk, bulk_dyn_smem<Q, T, 2>(), st>>>(a, gmap, fmap);
     else if (path == SSMD_PATH_SLAB)
-        bulk_kernel<Q, T, T, 3><<<nblk, blk, bulk_dyn_smem<Q, T, 3>(), st>>>(a, gmap, fmap);
+        bulk_kernel<Q, T, TG, 3><<<nblk, blk, bulk_dyn_smem<Q, T, 3>(), st>>>(a, gmap, fmap);
     else
-        bulk_kernel<Q, T, T, 1><<<nblk, blk, 0, st>>>(a, gmap, fmap);
+        bulk_kernel<Q, T, TG, 1><<<nblk, blk, 0, st>>>(a, gmap, fmap);
     if (ev1) cudaEventRecord(ev1, st);
     if (int e = cuda_check(cudaGetLastError(), "bulk_kernel launch")) return e;
 
@@ -312,15 +314,15 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
         // the two z faces are independent: one launch (reference order otherwise)
         dim3 g = grid2(G.nx, G.ny);
         g.z = 2;
-        bc_jet_z<Q, T, T><<<g, b2, 0, st>>>(a);
+        bc_jet_z<Q, T, TG><<<g, b2, 0, st>>>(a);
     } else {
-        if (G.bcy == BC_JET) bc_water_inflow<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
-        if (G.bcz == BC_JET) bc_oil_inflow<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
-        if (G.bcy == BC_JET) bc_outflow_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
-        if (G.bcz == BC_JET) bc_outflow_z<Q, T, T><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+        if (G.bcy == BC_JET) bc_water_inflow<Q, T, TG><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+        if (G.bcz == BC_JET) bc_oil_inflow<Q, T, TG><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
+        if (G.bcy == BC_JET) bc_outflow_y<Q, T, TG><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+        if (G.bcz == BC_JET) bc_outflow_z<Q, T, TG><<<grid2(G.nx, G.ny), b2, 0, st>>>(a);
     }
-    if (G.bcx == BC_COPY) bc_copy_x<Q, T, T><<<grid2(G.ny, G.nz), b2, 0, st>>>(a);
-    if (G.bcy == BC_COPY) bc_copy_y<Q, T, T><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
+    if (G.bcx == BC_COPY) bc_copy_x<Q, T, TG><<<grid2(G.ny, G.nz), b2, 0, st>>>(a);
+    if (G.bcy == BC_COPY) bc_copy_y<Q, T, TG><<<grid2(G.nx, G.nz), b2, 0, st>>>(a);
     if (flags & SSMD_STEP_AVERAGE) {
         // the bulk kernel updated the fluid cells; the ghost layers follow, then t advances
         const unsigned nb = (unsigned)((G.cells + 255) / 256);
@@ -334,10 +336,11 @@ template <int Q, class T>
 int launch_init_pops(const ssmd_params &p, const LBMFields &fl, cudaStream_t st) {
     const Geometry G = make_geometry(p);
     const unsigned nb = (unsigned)((G.cells + 255) / 256);
-    init_populations_kernel<Q, T, T><<<nb, 256, 0, st>>>(G, make_fields(fl), static_cast<T *>(fl.f),
-                                                          static_cast<T *>(p.f_alt),
-                                                          static_cast<T *>(fl.g),
-                                                          static_cast<T *>(p.g_alt));
+    using TG = phase_t<T>;
+    init_populations_kernel<Q, T, TG><<<nb, 256, 0, st>>>(G, make_fields(fl), static_cast<T *>(fl.f),
+                                                           static_cast<T *>(p.f_alt),
+                                                           static_cast<TG *>(fl.g),
+                                                           static_cast<TG *>(p.g_alt));
     return cuda_check(cudaGetLastError(), "init_populations launch");
 }
 

@@ -66,7 +66,7 @@ template <class T>
 int reduce_static(const ssmd_params &p, const LBMFields &fl, uint64_t steps_done, double *out_host,
                   cudaStream_t st) {
     const Geometry G = make_geometry(p);
-    const T *g = static_cast<const T *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
+    const phase_t<T> *g = static_cast<const phase_t<T> *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
     const uint64_t want = (G.cells + kRedThreads - 1) / kRedThreads;
     const int nb = (int)(want < (uint64_t)kStaticPartials ? want : kStaticPartials);
     if (nb > kStaticPartials)
@@ -76,7 +76,7 @@ int reduce_static(const ssmd_params &p, const LBMFields &fl, uint64_t steps_done
     if (int e = scratch_address(&scratch)) return e;
     double *partials = scratch;
     double *result = scratch + (size_t)kRedVals * kStaticPartials;
-    reduce_pass1<T><<<nb, kRedThreads, 0, st>>>(G, make_fields(fl), g, partials);
+    reduce_pass1<phase_t<T>><<<nb, kRedThreads, 0, st>>>(G, make_fields(fl), g, partials);
     reduce_pass2<<<1, kRedThreads, 0, st>>>(partials, nb, result);
     if (int e = cuda_check(cudaGetLastError(), "static reduce launch")) return e;
     if (int e = cuda_check(cudaMemcpyAsync(out_host, result, sizeof(double) * kRedVals,

@@ -76,13 +76,13 @@ template <class T>
 int launch_reduce(const ssmd_params &p, const LBMFields &fl, uint64_t steps_done, double *out_host,
                   cudaStream_t st) {
     const Geometry G = make_geometry(p);
-    const T *g = static_cast<const T *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
+    const phase_t<T> *g = static_cast<const phase_t<T> *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
     uint64_t nb64 = (G.cells + kRedThreads - 1) / kRedThreads;
     const int nb = (int)(nb64 < (uint64_t)kMaxRedBlocks ? nb64 : kMaxRedBlocks);
     char *ws = static_cast<char *>(p.workspace);
     double *partials = reinterpret_cast<double *>(ws + kPartialOff);
     double *out = reinterpret_cast<double *>(ws + kRedOutOff);
-    reduce_pass1<T><<<nb, kRedThreads, 0, st>>>(G, make_fields(fl), g, partials);
+    reduce_pass1<phase_t<T>><<<nb, kRedThreads, 0, st>>>(G, make_fields(fl), g, partials);
     reduce_pass2<<<1, kRedThreads, 0, st>>>(partials, nb, out);
     if (int e = cuda_check(cudaGetLastError(), "reduce launch")) return e;
     if (int e = cuda_check(cudaMemcpyAsync(out_host, out, sizeof(double) * kRedVals,

@@ -276,9 +276,11 @@ extern "C" int ssmd_phase_flux(const ssmd_params *p, const LBMFields *fields, ui
     switch (p->storage) {
     case SSMD_STORAGE_F32: phase_flux_kernel<float><<<nb, 256, 0, st>>>(G, static_cast<const float *>(g), acc); break;
     case SSMD_STORAGE_F16: phase_flux_kernel<__half><<<nb, 256, 0, st>>>(G, static_cast<const __half *>(g), acc); break;
-    default:
-        phase_flux_kernel<__nv_bfloat16><<<nb, 256, 0, st>>>(G, static_cast<const __nv_bfloat16 *>(g), acc);
+    default: { // BF16 runs keep g in half
+        using TG = phase_t<__nv_bfloat16>;
+        phase_flux_kernel<TG><<<nb, 256, 0, st>>>(G, static_cast<const TG *>(g), acc);
         break;
+    }
     }
     if (int e = cuda_check(cudaGetLastError(), "flux launch")) return e;
     double h[2] = {0.0, 0.0};

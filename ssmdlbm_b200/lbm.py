@@ -20,6 +20,10 @@ from ._lib import LBMFields, Params, Stats, check, lib
 
 STORAGE_DTYPES = {_lib.STORAGE_F32: torch.float32, _lib.STORAGE_F16: torch.float16,
                   _lib.STORAGE_BF16: torch.bfloat16}
+# element type of the phase populations g: BF16 runs keep g in half (phi in
+# [0, 1] needs mantissa bits, not range)
+PHASE_DTYPES = {_lib.STORAGE_F32: torch.float32, _lib.STORAGE_F16: torch.float16,
+                _lib.STORAGE_BF16: torch.float16}
 SCALARS = ("rho", "ux", "uy", "uz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz", "phi", "fsx", "fsy", "fsz")
 
 
@@ -49,9 +53,10 @@ class Simulation:
         Q = int(self.p.velocity_set)
         self.t = {k: torch.zeros(n, dtype=torch.float32, device=self.device) for k in SCALARS}
         self.t["f"] = torch.zeros(Q * n, dtype=dt, device=self.device)
-        self.t["g"] = torch.zeros(7 * n, dtype=dt, device=self.device)
+        dg = PHASE_DTYPES[self.p.storage]
+        self.t["g"] = torch.zeros(7 * n, dtype=dg, device=self.device)
         self.t["f_alt"] = torch.zeros(Q * n, dtype=dt, device=self.device)
-        self.t["g_alt"] = torch.zeros(7 * n, dtype=dt, device=self.device)
+        self.t["g_alt"] = torch.zeros(7 * n, dtype=dg, device=self.device)
         wsb = int(lib().ssmd_workspace_bytes(ctypes.byref(self.p)))
         self.t["workspace"] = torch.zeros(wsb, dtype=torch.uint8, device=self.device)
         self.fields = LBMFields()
@@ -221,7 +226,7 @@ class Simulation:
     def populations_push(self, which: int = 0) -> np.ndarray:
         """Current f (which=0) or g (which=1) in the reference's push layout, [q][z][y][x] float32."""
         Q = int(self.p.velocity_set) if which == 0 else 7
-        dt = STORAGE_DTYPES[self.p.storage]
+        dt = (STORAGE_DTYPES if which == 0 else PHASE_DTYPES)[self.p.storage]
         out = torch.empty(Q * self.cells, dtype=dt, device=self.device)
         torch.cuda.synchronize(self.device)
         check(lib().ssmd_populations_to_push(ctypes.byref(self.p), ctypes.byref(self.fields),

@@ -5,8 +5,10 @@ arithmetic throughout) against the same run in FP64 on the host.
 
 The bar for FP16 storage is 1 % on the centreline velocity and the phi mass.
 Measured on B200 (errors relative to the FP64 run): FP32 8e-5 / 2e-6 / 5e-8,
-FP16 2.4e-4 / 2.5e-4 / 4.3e-4, BF16 2.6e-2 / 1.8e-2 / 6.4e-3 (centreline
-u_z, centreline phi, phi mass)."""
+FP16 2.4e-4 / 2.5e-4 / 4.3e-4, BF16 2.5e-2 / 1.4e-2 / 6.2e-4 (centreline
+u_z, centreline phi, phi mass; BF16 runs keep the phase populations in half,
+so their phi mass is conserved like FP16's while u_z carries BF16's 8-bit
+mantissa)."""
 import numpy as np
 import pytest
 
@@ -42,7 +44,7 @@ def _rel(a, b):
 @pytest.mark.parametrize("storage,tol_uz,tol_phi,tol_mass", [
     (_lib.STORAGE_F32, 1e-3, 1e-4, 1e-6),
     (_lib.STORAGE_F16, 1e-2, 1e-2, 1e-2),   # the 1 % bar
-    (_lib.STORAGE_BF16, 6e-2, 4e-2, 2e-2),  # 8-bit mantissa: reported, not held to 1 %
+    (_lib.STORAGE_BF16, 6e-2, 4e-2, 5e-3),  # f's 8-bit mantissa: u_z reported, not held to 1 %
 ])
 def test_jet_statistics_vs_fp64_oracle(fp64_run, storage, tol_uz, tol_phi, tol_mass):
     from ssmdlbm_b200.lbm import Simulation
