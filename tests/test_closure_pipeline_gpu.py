@@ -38,3 +38,18 @@ def test_coarse_params_scaling():
     mob_c = (1 / q.omega_g - 0.5) * 0.25
     assert abs(mob_c - mob_f / 2) < 1e-6
     assert q.u_oil == p.u_oil and q.closure is None
+
+
+def test_fine_centreline_covers_the_coarse_sample():
+    """The fine run's centreline is averaged over the fine cells under the
+    coarse cells the coarse run samples (fine 2i, 2i + 1 under coarse i)."""
+    from ssmdlbm_b200 import closure
+    assert closure._coarse_axis_cells(31.5) == [31, 32]  # centred nozzle, even coarse size
+    assert closure._coarse_axis_cells(15.0) == [15]      # a nozzle on a cell centre
+    p = configs.oil_jet(128, 96, 256, 19, diam=16)
+    q = closure.coarse_params(p)
+    xs = [2 * i + 0.5 for i in closure._coarse_axis_cells(float(q.oil_cx))]
+    ys = [2 * j + 0.5 for j in closure._coarse_axis_cells(float(q.oil_cy))]
+    # the 2 x 2 fine blocks tile a 4 x 4 patch centred on the fine nozzle axis
+    assert xs == [62.5, 64.5] and abs(np.mean(xs) - float(p.oil_cx)) < 1e-6
+    assert ys == [46.5, 48.5] and abs(np.mean(ys) - float(p.oil_cy)) < 1e-6
