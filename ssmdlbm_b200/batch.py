@@ -93,9 +93,17 @@ class Sweep:
     def timed_one_by_one(self, steps: int) -> float:
         """Device seconds of the same steps issued lattice by lattice (one
         ssmd_step per lattice and step, one stream): the launch pattern a
-        sweep takes without the batched kernels."""
+        sweep takes without the batched kernels, each lattice with the
+        library's own z chunk (tile_z 0; the batched chunk does not carry
+        over, since a lattice launched alone needs enough work items of its
+        own)."""
         L = lib()
-        args = [(ctypes.byref(s.fields), ctypes.byref(self.params[i])) for i, s in enumerate(self.sims)]
+        singles = []
+        for pr in self.params:
+            q = pr.copy()
+            q.tile_z = 0
+            singles.append(q)
+        args = [(ctypes.byref(s.fields), ctypes.byref(singles[i])) for i, s in enumerate(self.sims)]
         self.sync()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(self.torch_stream)
