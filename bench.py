@@ -228,11 +228,15 @@ NCU_BYTES_PER_CELL = {(27, "f32"): 278.5, (19, "f32"): 214.4, (27, "f16"): 133.7
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
-    """Device time of `steps` steps replayed as 2-step graphs on this rank,
+    """Device time of exactly `steps` steps after exactly `warmup` untimed
+    ones, replayed as 2-step graphs (an odd count ends with one plain step),
     bracketed by barriers (replica_mlups takes the max over ranks)."""
     import torch
     sim.graph(2)
-    sim.run_graph(max(1, warmup // 2), 2)
+    sim.run_graph(warmup // 2, 2)
+    if warmup % 2:
+        sim.step(1)
+    sim.graph(2)  # captured for the parity the timed steps start at, outside the timing
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -240,6 +244,8 @@ def time_graph(sim, steps: int, warmup: int, world: int):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(s)
     sim.run_graph(steps // 2, 2)
+    if steps % 2:
+        sim.step(1)
     e1.record(s)
     e1.synchronize()
     barrier(world)
@@ -696,9 +702,7 @@ def main() -> int:
     if a.size:
         global NX, NY, NZ
         NX, NY, NZ = (int(v) for v in a.size.split(","))
-    if a.steps % 2:
-        a.steps += 1
-    a.warmup = max(a.warmup, 4)
+    a.warmup = max(a.warmup, 3)  # at least 3 untimed steps
     world, rank, local = dist_setup(a.gpus)
     if a.impl == "reference":
         line = run_reference(a, world, rank)
