@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NX, NY, NZ = 128, 128, 512
+# the reference's only published figures for the path: MLUPS of the full step,
+# D3Q19 / D3Q27 + D3Q7, on an RTX 3050 (its README; lattice size not stated)
+PUBLISHED_MLUPS = {19: 440.0, 27: 377.0}
 Q = 27
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -615,7 +618,11 @@ def run_ours(a, world, rank, local):
     line = {
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt * 1e3 / a.steps, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": round(value / PUBLISHED_MLUPS[a.vs], 2),
+        "vs_baseline_note": (f"the reference's published {PUBLISHED_MLUPS[a.vs]} MLUPS for D3Q{a.vs}+D3Q7 "
+                             "(its README, RTX 3050, lattice size not stated)"),
+        "dtype": "f32",
         "data": "synthetic: quiescent water + noisy oil inlet (the reference's initial state)",
         "config": {"workload": f"oil jet D3Q{a.vs}+D3Q7 {NX}x{NY}x{NZ}, {a.storage} storage, nozzle 16, "
                                "tau 0.52, w 0.05 + 1% noise, seed 1",
@@ -664,7 +671,7 @@ def run_reference(a, world, rank):
     return {
         "metric": "MLUPS", "value": round(v, 1), "unit": "MLUPS", "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "vs_baseline": round(v / PUBLISHED_MLUPS[27], 2), "dtype": "f32", "impl": "reference",
         "data": "synthetic: the reference's own initial state",
         "config": {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, FP32 storage, nozzle 16, tau 0.52 "
                                "(reference build: no noise, nozzle at (nx-1)/2, (ny-1)/4, M = 0.125)",
