@@ -502,8 +502,9 @@ struct Bulk {
     //   A = nx(+1, 0) - nx(-1, 0) + ny(0, +1) - ny(0, -1)
     //   B = sum over the 4 corners (dx, dy) of dx nx + dy ny
     // (w3 = 0 for D3Q19).  Every thread evaluates them once per plane for its
-    // own column and keeps the previous planes in registers, so the cell
-    // update reads 4 normal values instead of the full 3 x 3 x 3 stencil.
+    // own column and keeps those of the previous planes in its column of
+    // shared memory (Curv), so the cell update combines three carried sums
+    // instead of reading the full 3 x 3 x 3 stencil of normals.
     static __device__ __forceinline__ void plane_terms(const BulkSmem &S, int pz, int tx, int ty, float &C,
                                                        float &Sv, float &Zv) {
         const int s = ringN(pz);
