@@ -9,6 +9,8 @@ FP16 2.4e-4 / 2.5e-4 / 4.3e-4, BF16 2.5e-2 / 1.4e-2 / 6.2e-4 (centreline
 u_z, centreline phi, phi mass; BF16 runs keep the phase populations in half,
 so their phi mass is conserved like FP16's while u_z carries BF16's 8-bit
 mantissa)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -62,3 +64,47 @@ def test_jet_statistics_vs_fp64_oracle(fp64_run, storage, tol_uz, tol_phi, tol_m
     assert errs["centreline_uz"] <= tol_uz, errs
     assert errs["centreline_phi"] <= tol_phi, errs
     assert errs["phi_mass"] <= tol_mass, errs
+
+
+# ---------------------------------------------------------------------------
+# The 128 x 128 x 512 D3Q27 jet (nozzle 16, tau 0.52, seed 1) after 1000 steps
+# against the FP64 oracle's statistics in tests/golden/c2_fp64_1000.npz, made by
+# tests/golden/make_c2_fp64.py on the host cores (an hour of FP64 work, so the
+# fixture stands in for a live oracle run).
+GOLDEN_C2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_fp64_1000.npz")
+C2_TOLERANCES = [  # centreline u_z, centreline phi, phi mass, volume of the phi > 1/2 components
+    (_lib.STORAGE_F32, 1e-1, 1e-1, 1e-1, 1e-1),
+    (_lib.STORAGE_F16, 1e-1, 1e-1, 1e-1, 1e-1),
+    (_lib.STORAGE_BF16, 1e-1, 1e-1, 1e-1, 1e-1),
+]
+
+
+def _c2_params(storage):
+    return configs.oil_jet(128, 128, 512, 27, tau=0.52, sigma=1e-3, width=4.0, mobility=0.1, diam=16,
+                           w_in=0.05, noise=0.01, seed=1, storage=storage)
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("storage,tol_uz,tol_phi,tol_mass,tol_vol", C2_TOLERANCES)
+def test_c2_jet_statistics_vs_fp64_fixture(storage, tol_uz, tol_phi, tol_mass, tol_vol):
+    from ssmdlbm_b200.lbm import Simulation
+    g = np.load(GOLDEN_C2)
+    sim = Simulation(_c2_params(storage))
+    sim.init()
+    sim.step(int(g["steps"]), store_macros=True)
+    assert sim.check_status() == 0
+    uz, phi = sim.centreline()
+    mass = float(sim.field("phi").astype(np.float64)[1:-1].sum())
+    d = sim.droplets(0.5)
+    errs = {"centreline_uz": _rel(uz, g["uz"]), "centreline_phi": _rel(phi, g["phi"]),
+            "phi_mass": abs(mass - float(g["mass"])) / float(g["mass"]),
+            "phi_gt_half_volume": abs(float(d["volume"].sum()) - float(g["drop_volume"].sum()))
+            / float(g["drop_volume"].sum())}
+    print(storage, errs)
+    # the same components: their number, and which of them touch the inlet plane
+    assert len(d) == len(g["drop_volume"])
+    assert sorted(d["touches_inlet"].tolist()) == sorted(g["drop_touch"].tolist())
+    assert errs["centreline_uz"] <= tol_uz, errs
+    assert errs["centreline_phi"] <= tol_phi, errs
+    assert errs["phi_mass"] <= tol_mass, errs
+    assert errs["phi_gt_half_volume"] <= tol_vol, errs
