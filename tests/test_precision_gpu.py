@@ -70,12 +70,14 @@ def test_jet_statistics_vs_fp64_oracle(fp64_run, storage, tol_uz, tol_phi, tol_m
 # The 128 x 128 x 512 D3Q27 jet (nozzle 16, tau 0.52, seed 1) after 1000 steps
 # against the FP64 oracle's statistics in tests/golden/c2_fp64_1000.npz, made by
 # tests/golden/make_c2_fp64.py on the host cores (an hour of FP64 work, so the
-# fixture stands in for a live oracle run).
+# fixture stands in for a live oracle run).  Measured on B200 (u_z, phi, phi
+# mass, phi > 1/2 volume): FP32 1.6e-5 / 2.0e-6 / 2.6e-7 / 2.7e-7, FP16
+# 1.7e-3 / 1.5e-4 / 2.2e-4 / 9.6e-5, BF16 2.8e-2 / 1.6e-2 / 1.3e-4 / 1.5e-4.
 GOLDEN_C2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_fp64_1000.npz")
 C2_TOLERANCES = [  # centreline u_z, centreline phi, phi mass, volume of the phi > 1/2 components
-    (_lib.STORAGE_F32, 1e-1, 1e-1, 1e-1, 1e-1),
-    (_lib.STORAGE_F16, 1e-1, 1e-1, 1e-1, 1e-1),
-    (_lib.STORAGE_BF16, 1e-1, 1e-1, 1e-1, 1e-1),
+    (_lib.STORAGE_F32, 1e-4, 1e-5, 2e-6, 2e-6),
+    (_lib.STORAGE_F16, 1e-2, 1e-2, 1e-2, 1e-2),   # the 1 % bar
+    (_lib.STORAGE_BF16, 6e-2, 4e-2, 2e-3, 2e-3),  # f's 8-bit mantissa: u_z reported, not held to 1 %
 ]
 
 
