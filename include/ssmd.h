@@ -313,14 +313,19 @@ int ssmd_reduce(const ssmd_params *p, const LBMFields *fields, uint64_t steps_do
  * ssmd_reduce without any device allocation.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a plugin handed
  * the fields by the host application with no memory of its own, or code that
- * must not call cudaMalloc because it synchronises the device or a capture is
- * open): p->workspace is not used; the partial sums live in a fixed 41 KiB
- * array inside the library (512 partials of 10 doubles + result, per GPU,
- * held until exit).  Every lattice ssmd_validate accepts fits; a larger
- * partial count is refused.  The first call on a device looks the array up
- * (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array: overlapping calls race.  Same results as ssmd_reduce
- * up to FP64 summation order; synchronises the stream.
+ * must not call cudaMalloc because it synchronises the whole device):
+ * p->workspace is not used; the partial sums live in a fixed 41 KiB array
+ * inside the library (512 partials of 10 doubles + result, per GPU, held
+ * until exit).  512 blocks striding over the cells cover every lattice that
+ * ssmd_validate accepts; larger lattices are refused by ssmd_validate.  The
+ * first call in each CUDA context of a device looks the array up
+ * (cudaGetSymbolAddress); after a device reset the next call looks it up
+ * again.  The call reads its result back and synchronises the stream, so it
+ * cannot be captured: a capturing stream is refused with
+ * SSMD_ERR_INVALID_ARGUMENT, and it must not be called on the legacy default
+ * stream while another stream captures.  All calls share the array:
+ * overlapping calls race.  Same results as ssmd_reduce up to FP64 summation
+ * order.
  */
 int ssmd_reduce_static(const ssmd_params *p, const LBMFields *fields, uint64_t steps_done,
                        ssmd_stats *out, ssmd_stream_t stream);

@@ -11,8 +11,15 @@
   the include path, plus oracle/ref_harness/harness.cu as the driver.  The
   nvcc flags are those of the reference's compile.sh:58-75 (minus the
   lto/-rdc pair, which only matters for multi-file device linking) with the
-  case's velocity set and ENABLE_FP16.  Needs /root/reference (this
-  container); the built binaries travel with the repository copy.
+  case's velocity set and ENABLE_FP16.  The built binaries travel with the
+  repository copy; building them needs the reference's checkout.
+
+Where the reference's sources are: the environment variable SSMD_REFERENCE
+names the root of a checkout of brenogemelgo/ssmdLBM (the directory that
+holds its compile.sh and src/); without it the recipe looks in
+/root/reference, the read-only checkout of the machine these builds were
+first made on.  When neither holds src/lbm.cu the reference binaries are
+skipped (build_ref returns an empty list).
 """
 from __future__ import annotations
 
@@ -24,7 +31,8 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_SRC = "/root/reference/src"
+REF_ROOT = os.environ.get("SSMD_REFERENCE", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
 ORACLE_SO = os.path.join(HERE, "_build", "libssmd_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
@@ -135,7 +143,7 @@ def build_vti_case(case: str, force: bool = False) -> str:
 
 
 def build_ref(force: bool = False) -> list[str]:
-    if not os.path.isdir(REF_SRC):
+    if not os.path.isfile(os.path.join(REF_SRC, "lbm.cu")):
         return []
     with cf.ThreadPoolExecutor(max_workers=min(8, len(CASES))) as ex:
         out = list(ex.map(lambda k: build_ref_case(k, force), CASES))

@@ -8,9 +8,13 @@
 // both buffers: slots no kernel writes are identical in the two, every other
 // slot is rewritten before it is read.
 //
-// File: 64-byte header {magic "SSMDCKP1", abi, sizeof(ssmd_params),
+// File: 64-byte header {magic "SSMDCKP2", abi, sizeof(ssmd_params),
 // steps_done, device step, cells, Q, storage} + ssmd_params (pointers
 // cleared) + 11 FP32 arrays (rho ux uy uz pxx pyy pzz pxy pxz pyz phi) + f + g.
+// Format 2 stores g of BF16-storage lattices as IEEE half (format 1 stored
+// bfloat16); loading refuses format-1 files and any header whose ABI version,
+// cell count, velocity set or storage differs from the caller's parameters,
+// so a file is never read with the wrong element types.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -36,6 +40,7 @@ struct Header {
     uint64_t reserved[2];
 };
 static_assert(sizeof(Header) == 64, "checkpoint header is 64 bytes");
+constexpr char kMagic[9] = "SSMDCKP2";
 
 float *const *scalar_list(const LBMFields *f, float *(&out)[11]) {
     float *v[11] = {f->rho, f->ux, f->uy, f->uz, f->pxx, f->pyy, f->pzz, f->pxy, f->pxz, f->pyz, f->phi};
@@ -62,7 +67,7 @@ extern "C" int ssmd_checkpoint_save(const ssmd_params *p, const LBMFields *field
     std::FILE *fp = std::fopen(path, "wb");
     if (!fp) return fail(SSMD_ERR_INVALID_ARGUMENT, "cannot open %s", path);
     Header h{};
-    std::memcpy(h.magic, "SSMDCKP1", 8);
+    std::memcpy(h.magic, kMagic, 8);
     h.abi = SSMD_ABI_VERSION;
     h.params_bytes = sizeof(ssmd_params);
     h.steps_done = steps_done;
@@ -101,11 +106,18 @@ extern "C" int ssmd_checkpoint_load(const ssmd_params *p, LBMFields *fields, con
     if (!fp) return fail(SSMD_ERR_INVALID_ARGUMENT, "cannot open %s", path);
     Header h{};
     ssmd_params pc{};
-    bool ok = std::fread(&h, sizeof h, 1, fp) == 1 && std::memcmp(h.magic, "SSMDCKP1", 8) == 0 &&
-              h.params_bytes == sizeof(ssmd_params) && std::fread(&pc, sizeof pc, 1, fp) == 1;
+    bool ok = std::fread(&h, sizeof h, 1, fp) == 1;
+    if (ok && std::memcmp(h.magic, "SSMDCKP", 7) == 0 && std::memcmp(h.magic, kMagic, 8) != 0) {
+        std::fclose(fp);
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "%s is a checkpoint of an older format (%.8s, this library reads %.8s)",
+                    path, h.magic, kMagic);
+    }
+    ok = ok && std::memcmp(h.magic, kMagic, 8) == 0 && h.abi == SSMD_ABI_VERSION &&
+         h.params_bytes == sizeof(ssmd_params) && h.cells == (uint64_t)p->nx * p->ny * p->nz &&
+         h.q == p->velocity_set && h.storage == p->storage && std::fread(&pc, sizeof pc, 1, fp) == 1;
     if (!ok || !same_problem(pc, *p)) {
         std::fclose(fp);
-        return fail(SSMD_ERR_INVALID_ARGUMENT, "%s is not a checkpoint of this lattice / storage", path);
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "%s is not a checkpoint of this lattice / storage / ABI", path);
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (int e = cuda_check(cudaStreamSynchronize(st), "checkpoint sync")) {

@@ -4,26 +4,32 @@
 // buffer.  Some callers cannot provide one: a monitoring or post-processing
 // plugin that is handed the simulation's LBMFields by the host application
 // but owns no device memory of its own, or code running where cudaMalloc is
-// off limits (it synchronises the whole device and is illegal while a stream
-// is being captured).  ssmd_reduce_static serves them: the same two reduction
-// kernels, with the partial sums and the result in a fixed array that lives
-// in this library's own device image.
+// off limits (it synchronises the whole device).  ssmd_reduce_static serves
+// them: the same two reduction kernels, with the partial sums and the result
+// in a fixed array that lives in this library's own device image.
 //
 // Limits and sharing rules:
 //   * the array holds kStaticPartials = 512 partial sums of kRedVals doubles
 //     plus one result row (41 KiB per GPU that loads the library, held until
 //     the process exits).  The first pass launches at most 512 blocks that
-//     stride over the cells, so every lattice the library accepts
-//     (nx*ny*nz <= 2^32 - 1, checked by ssmd_validate) fits; a partial count
-//     above 512 is refused with SSMD_ERR_INVALID_ARGUMENT.
+//     stride over the cells, so 512 partials cover every lattice that
+//     ssmd_validate accepts (nx*ny*nz <= 2^32 - 1); larger lattices are
+//     refused by ssmd_validate before anything reaches the device.
 //   * every call on a device uses the same array and leaves its contents
 //     behind.  Pass 1 overwrites every partial that pass 2 reads and pass 2
 //     overwrites the result row, so nothing has to start at zero.  Calls that
 //     overlap on the GPU (different streams or threads at the same time) race
 //     on the array and corrupt each other's results: serialise them.
-//   * the device address of the array is looked up once per device with
-//     cudaGetSymbolAddress on the first call made while that device is
-//     current; make that first call before any stream capture.
+//   * the call copies its result to the host and synchronises its stream, so
+//     it cannot run inside a stream capture: a capturing stream is refused
+//     with SSMD_ERR_INVALID_ARGUMENT, and it must not be called on the legacy
+//     default stream while another stream of the device is being captured.
+//   * the device address of the array is looked up with cudaGetSymbolAddress
+//     on the first call in each CUDA context of a device (the device that is
+//     current) and kept for later calls in the same context.  A device reset
+//     or a released and re-created primary context gives a new context, in
+//     which the next call looks the address up again.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -37,28 +43,71 @@ namespace {
 
 constexpr int kStaticPartials = 512;
 constexpr int kMaxDevices = 64;
+// ceil(cells / kRedThreads) blocks, clamped to kStaticPartials: pass 1 strides
+// over the cells, so the clamp only lengthens each block's loop
+static_assert(kStaticPartials <= kMaxRedBlocks, "pass 2 sums at most kMaxRedBlocks partial rows");
 
 // [0, kRedVals * kStaticPartials): partials; last kRedVals doubles: result.
 static __device__ __align__(256) double g_reduce_scratch[kRedVals * (kStaticPartials + 1)];
 
-std::mutex g_setup_mutex;
-double *g_scratch_ptr[kMaxDevices] = {};
+// Unique ID of the calling thread's current CUDA context (0 when none is
+// current yet or the driver entry points are unavailable).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
 
-// Device address of g_reduce_scratch on the current device (set-up on first use).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+struct ScratchCache {
+    unsigned long long ctx_id = 0; // context the address belongs to (0: none cached)
+    double *ptr = nullptr;
+};
+
+std::mutex g_setup_mutex;
+ScratchCache g_scratch[kMaxDevices];
+
+// Device address of g_reduce_scratch in the current device's current context.
 int scratch_address(double **out) {
     int dev = 0;
     if (int e = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return e;
     if (dev < 0 || dev >= kMaxDevices)
         return fail(SSMD_ERR_UNSUPPORTED, "device index %d above %d", dev, kMaxDevices - 1);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *ptr = nullptr;
-        if (int e = cuda_check(cudaGetSymbolAddress(&ptr, g_reduce_scratch),
-                               "cudaGetSymbolAddress(reduction scratch)"))
-            return e;
-        g_scratch_ptr[dev] = static_cast<double *>(ptr);
+    ScratchCache &c = g_scratch[dev];
+    const unsigned long long id = current_context_id();
+    if (id != 0 && c.ctx_id == id && c.ptr) {
+        *out = c.ptr;
+        return SSMD_OK;
     }
-    *out = g_scratch_ptr[dev];
+    // set-up for this device and context: the runtime makes the device's
+    // primary context current here if nothing was current yet
+    void *ptr = nullptr;
+    if (int e = cuda_check(cudaGetSymbolAddress(&ptr, g_reduce_scratch),
+                           "cudaGetSymbolAddress(reduction scratch)"))
+        return e;
+    c.ptr = static_cast<double *>(ptr);
+    c.ctx_id = id != 0 ? id : current_context_id(); // 0 again: no cache, look up on every call
+    *out = c.ptr;
     return SSMD_OK;
 }
 
@@ -69,9 +118,6 @@ int reduce_static(const ssmd_params &p, const LBMFields &fl, uint64_t steps_done
     const phase_t<T> *g = static_cast<const phase_t<T> *>((steps_done & 1ull) == 0ull ? fl.g : p.g_alt);
     const uint64_t want = (G.cells + kRedThreads - 1) / kRedThreads;
     const int nb = (int)(want < (uint64_t)kStaticPartials ? want : kStaticPartials);
-    if (nb > kStaticPartials)
-        return fail(SSMD_ERR_INVALID_ARGUMENT, "reduction needs %d partial sums, static scratch holds %d",
-                    nb, kStaticPartials);
     double *scratch = nullptr;
     if (int e = scratch_address(&scratch)) return e;
     double *partials = scratch;
@@ -96,6 +142,12 @@ extern "C" int ssmd_reduce_static(const ssmd_params *p, const LBMFields *fields,
     for (const void *q : need)
         if (!q) return fail(SSMD_ERR_INVALID_ARGUMENT, "a field, g or g_alt pointer is null");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (int e = cuda_check(cudaStreamIsCapturing(st, &cap), "cudaStreamIsCapturing")) return e;
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(SSMD_ERR_INVALID_ARGUMENT,
+                    "ssmd_reduce_static synchronises its stream and cannot be captured: call it on a stream "
+                    "that is not being captured");
     double v[kRedVals];
     int e;
     switch (p->storage) {

@@ -138,3 +138,43 @@ def test_oil_jet_parameters():
     assert abs(p.gamma - 4 * 0.1 / (4 * 0.25)) < 1e-7
     assert p.oil_r2 == 16.0 and p.oil_cx == 31.5 and p.oil_cy == 31.5
     assert lib().ssmd_validate(ctypes.byref(p)) == 0
+
+
+def _fake_fields_and_params(q=19, storage=_lib.STORAGE_F32):
+    """Parameters and non-null placeholder pointers that pass the host checks;
+    the calls below must refuse before any of them is dereferenced."""
+    p = _lib.reference_params(32, 32, 64, q)
+    p.storage = storage
+    f = LBMFields()
+    for name, _ in LBMFields._fields_:
+        setattr(f, name, ctypes.c_void_p(0x1000))
+    p.f_alt = p.g_alt = p.workspace = ctypes.c_void_p(0x1000)
+    p.workspace_bytes = lib().ssmd_workspace_bytes(ctypes.byref(p))
+    return p, f
+
+
+def _checkpoint_header(magic=b"SSMDCKP2", abi=None, cells=32 * 32 * 64, q=19, storage=0):
+    import struct
+    abi = lib().ssmd_abi_version() if abi is None else abi
+    return struct.pack("<8sIIQQQii16s", magic, abi, ctypes.sizeof(Params), 0, 0, cells, q, storage, b"\0" * 16)
+
+
+@pytest.mark.parametrize("kw,fragment", [
+    (dict(magic=b"SSMDCKP1"), "older format"),
+    (dict(abi=999), "not a checkpoint"),
+    (dict(q=27), "not a checkpoint"),
+    (dict(storage=_lib.STORAGE_BF16), "not a checkpoint"),
+    (dict(cells=7), "not a checkpoint"),
+    (dict(magic=b"NOTACKPT"), "not a checkpoint"),
+])
+def test_checkpoint_load_refuses_other_formats_without_touching_the_device(tmp_path, kw, fragment):
+    """A checkpoint of another format, ABI, velocity set, storage or size is
+    refused from its header, before any device memory is read or written."""
+    p, f = _fake_fields_and_params()
+    path = tmp_path / "c.ckp"
+    path.write_bytes(_checkpoint_header(**kw) + bytes(ctypes.sizeof(Params)))
+    steps = ctypes.c_uint64(123)
+    rc = lib().ssmd_checkpoint_load(ctypes.byref(p), ctypes.byref(f), str(path).encode(), ctypes.byref(steps), None)
+    assert rc == _lib.SSMD_ERR_INVALID_ARGUMENT
+    assert fragment in lib().ssmd_last_error().decode()
+    assert steps.value == 123
