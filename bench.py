@@ -45,9 +45,17 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
-def b_alg(q: int, s_f: int) -> int:
-    """Compulsory bytes per cell update: read + write of f (q s_f), g (7 s_f) and phi (4)."""
-    return 2 * (q * s_f + 7 * s_f + 4)
+def b_alg(q: int, s_f: int, s_g: int | None = None) -> int:
+    """Compulsory bytes per cell update: read + write of f (q s_f), g (7 s_g,
+    s_g = s_f unless given) and phi (4)."""
+    return 2 * (q * s_f + 7 * (s_f if s_g is None else s_g) + 4)
+
+
+def element_sizes(storage: int) -> tuple:
+    """(bytes per f population, bytes per g population) of a storage kind."""
+    from ssmdlbm_b200 import _lib
+    return {_lib.STORAGE_F32: (4, 4), _lib.STORAGE_F16: (2, 2), _lib.STORAGE_BF16: (2, 2),
+            _lib.STORAGE_F16_G32: (2, 4)}[storage]
 
 
 def hbm_peak():
@@ -222,7 +230,7 @@ def workload(storage: int, q: int = Q):
                            w_in=0.05, noise=0.01, seed=1, storage=storage)
 
 
-STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2}
+STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2, "f16g32": 3}
 
 # DRAM bytes per cell of one bulk launch on the 128 x 128 x 512 jet,
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of that
@@ -375,39 +383,71 @@ def run_sweep(steps: int = 40):
     return out
 
 
-def mlp_throughput(rows: int = 1 << 20, reps: int = 20):
-    """Device throughput of the closure network (tensor-core kernels)."""
+def mlp_throughput(net=None, rows: int = 1 << 24, reps: int = 20):
+    """Device throughput of the closure network's kernels (CUDA events):
+    forward from a feature array, the gradient with atomics and with the
+    reproducible per-CTA reduction, and the fused refresh (features from the
+    fields, network, bounds) on the 192 x 192 x 768 coarse lattice.  FLOPs
+    are the network's multiply-adds, 2 (12 x 64 + 64 x 64 + 64 x 2) per row
+    forward and three times that for the gradient."""
+    import ctypes as ct
     import torch
-    from ssmdlbm_b200 import _lib
-    from ssmdlbm_b200.closure import Network
+    from ssmdlbm_b200 import _lib, closure
+    from ssmdlbm_b200.lbm import Simulation
     L = _lib.lib()
-    net = Network(0)
+    if net is None:
+        net = closure.Network(0)
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     feats = torch.randn(rows, _lib.MLP_IN, device="cuda", generator=g)
     tg = torch.rand(rows, 2, device="cuda", generator=g)
     out = torch.empty(rows, 2, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
-    res = {}
-    for name in ("forward", "grad"):
-        def once():
-            if name == "forward":
-                _lib.check(L.ssmd_mlp_forward(net.net.data_ptr(), feats.data_ptr(), rows, out.data_ptr(), st))
-            else:
-                _lib.check(L.ssmd_mlp_grad(net.net.data_ptr(), feats.data_ptr(), tg.data_ptr(), None, rows,
-                                           net.grad.data_ptr(), net.loss.data_ptr(), st))
+    n_ptr, g_ptr, l_ptr = net.net.data_ptr(), net.grad.data_ptr(), net.loss.data_ptr()
+
+    def timed(fn, n_reps):
         for _ in range(3):
-            once()
+            fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(reps):
-            once()
+        for _ in range(n_reps):
+            fn()
         e1.record()
         e1.synchronize()
-        s_per = e0.elapsed_time(e1) / 1e3 / reps
-        flop = 2 * (12 * 64 + 64 * 64 + 64 * 2) * rows * (1 if name == "forward" else 3)
-        res[name] = {"rows_per_s": round(rows / s_per / 1e9, 3), "unit": "G rows/s", "ms": round(s_per * 1e3, 4),
-                     "tflops": round(flop / s_per / 1e12, 2)}
+        return e0.elapsed_time(e1) / 1e3 / n_reps
+
+    flop_row = 2 * (12 * 64 + 64 * 64 + 64 * 2)
+    res = {}
+    calls = {
+        "forward": (lambda: _lib.check(L.ssmd_mlp_forward(n_ptr, feats.data_ptr(), rows, out.data_ptr(), st)), 1),
+        "grad_atomic": (lambda: _lib.check(L.ssmd_mlp_grad(n_ptr, feats.data_ptr(), tg.data_ptr(), None, rows, g_ptr,
+                                                            l_ptr, st)), 3),
+        "grad_reproducible": (lambda: _lib.check(L.ssmd_mlp_grad_ws(n_ptr, feats.data_ptr(), tg.data_ptr(), None, rows,
+                                                                     g_ptr, l_ptr, net.ws.data_ptr(),
+                                                                     net.ws.numel() * 4, st)), 3)}
+    for name, (fn, mult) in calls.items():
+        s_per = timed(fn, reps)
+        res[name] = {"rows": rows, "g_rows_per_s": round(rows / s_per / 1e9, 3), "ms": round(s_per * 1e3, 4),
+                     "tflops": round(flop_row * mult * rows / s_per / 1e12, 2)}
+    del feats, tg, out
+    cp = closure.coarse_params(c5_params())
+    cp.storage = _lib.STORAGE_F16
+    sim = Simulation(cp)
+    sim.init()
+    sim.step(2, store_macros=True)
+    n = sim.cells
+    nut, cs = torch.empty(n, device="cuda"), torch.empty(n, device="cuda")
+    pr, fl = ct.byref(sim.p), ct.byref(sim.fields)
+    s_per = timed(lambda: _lib.check(L.ssmd_closure_refresh(pr, fl, n_ptr, 0.05, nut.data_ptr(), cs.data_ptr(),
+                                                             sim.stream)), 10)
+    step_s = timed(lambda: sim.step(1), 10)
+    res["refresh_fused"] = {"cells": n, "g_cells_per_s": round(n / s_per / 1e9, 3), "ms": round(s_per * 1e3, 4),
+                            "tflops": round(flop_row * n / s_per / 1e12, 2),
+                            "coarse_step_ms": round(step_s * 1e3, 4),
+                            "bytes_per_cell": 28, "note": "reads rho, u, phi (20 B) and writes nu_t, sigma factor (8 B)"}
+    sim.close()
+    del sim
+    torch.cuda.empty_cache()
     return res
 
 
@@ -430,124 +470,171 @@ def stat_diffs(s: dict, ref: dict) -> dict:
                                if ref["droplet_volume"] > 0 else None)}
 
 
+C2_FP64 = os.path.join(ROOT, "tests", "golden", "c2_fp64_5000.npz")
+
+
 def run_precision(steps: int = 5000):
-    """The 128 x 128 x 512 D3Q27 jet for `steps` steps with FP32, shifted FP16
-    and shifted BF16 population storage (FP32 arithmetic in all three): the
-    16-bit runs' centreline u_z, centreline phi, phi mass and droplets against
-    the FP32 run's."""
+    """The 128 x 128 x 512 D3Q27 jet for `steps` steps with FP32, shifted
+    FP16, shifted BF16 and FP16-with-FP32-phase population storage (FP32
+    arithmetic in all four), judged by the FP64 oracle's statistics of the
+    same jet (tests/golden/c2_fp64_5000.npz, computed by the oracle's FP64
+    GPU instance): centreline u_z and phi, phi mass, the phi > 1/2 volume and
+    the droplet-size histogram."""
+    import numpy as np
     import torch
     from ssmdlbm_b200 import _lib
     from ssmdlbm_b200.lbm import Simulation
-    out, ref = {}, None
-    for name, stg in (("f32", _lib.STORAGE_F32), ("f16", _lib.STORAGE_F16), ("bf16", _lib.STORAGE_BF16)):
+    g = np.load(C2_FP64)
+    assert int(g["steps"]) == steps
+    rel = lambda a, b: float(np.linalg.norm(a[1:-1] - b[1:-1]) / np.linalg.norm(b[1:-1]))
+    out = {}
+    for name, stg in (("f32", _lib.STORAGE_F32), ("f16", _lib.STORAGE_F16), ("bf16", _lib.STORAGE_BF16),
+                      ("f16_g32", _lib.STORAGE_F16_G32)):
         sim = Simulation(workload(stg, 27))
         sim.init()
         sim.step(steps, store_macros=True)
-        st = jet_stats(sim)
+        uz, phi = sim.centreline()
+        mass = float(sim.field("phi").astype(np.float64)[1:-1].sum())
+        d = sim.droplets(0.5)
+        hist = np.histogram(np.asarray(d["volume"], np.float64), bins=g["hist_edges"])[0]
+        out[name + "_vs_fp64"] = {
+            "centreline_uz": rel(uz, g["uz"]), "centreline_phi": rel(phi, g["phi"]),
+            "phi_mass": abs(mass - float(g["mass"])) / float(g["mass"]),
+            "phi_gt_half_volume": abs(float(d["volume"].sum()) - float(g["drop_volume"].sum()))
+            / float(g["drop_volume"].sum()),
+            "components": [int(len(d)), int(len(g["drop_volume"]))],
+            "droplet_hist_l1": int(np.abs(hist - g["drop_hist"]).sum())}
         sim.close()
         del sim
         torch.cuda.empty_cache()
-        if ref is None:
-            ref = st
-            out["f32"] = {"droplets": st["droplets"], "phi_mass": st["mass"]}
-        else:
-            out[name + "_vs_f32"] = stat_diffs(st, ref)
     return {"workload": f"oil jet D3Q27+D3Q7 {NX}x{NY}x{NZ}, {steps} steps, nozzle 16, tau 0.52, seed 1",
-            "reference": "the FP32-storage run (same arithmetic); the FP64 oracle judges small lattices "
-                         "in tests/test_parity_gpu.py", **out}
+            "judge": "FP64 oracle (oracle_cells.h as FP64 CUDA kernels, bit-identical to the host build), "
+                     "statistics in tests/golden/c2_fp64_5000.npz", **out}
 
 
-def run_production(net, steps: int = 200, update_every: int = 10):
-    """Production lattice 384 x 384 x 1536 (226 M cells, D3Q27 + D3Q7, nozzle
-    24, w 0.06 + 1 % noise, seed 3, sigma 1e-3, tau 0.52): FP16 storage with
-    the learned closure (network from the closure leg, refreshed every
-    `update_every` steps) against the plain FP32 method, `steps` steps each."""
-    import ctypes as ct
+def c5_params():
+    """384 x 384 x 1536 D3Q27 + D3Q7 jet: nozzle 24, w 0.06 + 1 % noise (seed
+    3), sigma 1e-3, tau 0.52, interface width 4, mobility 0.1."""
+    from ssmdlbm_b200 import configs
+    return configs.oil_jet(384, 384, 1536, 27, tau=0.52, sigma=1e-3, width=4.0, mobility=0.1, diam=24,
+                           w_in=0.06, noise=0.01, seed=3)
+
+
+def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5000, train_steps: int = 20000,
+                   update_every: int = 10):
+    """The production jet: plain FP32 on the fine 384 x 384 x 1536 lattice
+    (the judge, and the source of the training data: filtered 2x onto
+    192 x 192 x 768 every `sample_every` steps from `spinup` on, the last
+    snapshot held out), the closure network trained on them (Adam, lr 1e-3,
+    batch 65536), then the coarse lattice with FP16 storage, plain and with
+    the closure refreshed every `update_every` coarse steps, for half the
+    steps (acoustic scaling).  Statistics are time averages over the same
+    snapshots, on the coarse cells."""
     import torch
-    from ssmdlbm_b200 import _lib, configs
+    from ssmdlbm_b200 import _lib, closure
     from ssmdlbm_b200.lbm import Simulation
-    L = _lib.lib()
     peak, _ = hbm_peak()
-    res = {"workload": f"oil jet D3Q27+D3Q7 384x384x1536, nozzle 24, w 0.06 + 1% noise, seed 3, {steps} steps; "
-                       f"FP16 + closure every {update_every} steps vs FP32 plain"}
-    stats = {}
-    for name, stg in (("f32_plain", _lib.STORAGE_F32), ("f16_closure", _lib.STORAGE_F16)):
-        p = configs.oil_jet(384, 384, 1536, 27, tau=0.52, sigma=1e-3, width=4.0, mobility=0.1, diam=24,
-                            w_in=0.06, noise=0.01, seed=3, storage=stg)
+    fine_p = c5_params()
+    r = closure.experiment(fine_p, steps=steps, sample_every=sample_every, spinup=spinup, train_steps=train_steps,
+                           batch=65536, lr=1e-3, seed=0, update_every=update_every, nut_max=0.05,
+                           coarse_storage=_lib.STORAGE_F16)
+    f, pl, cl = r["fine"], r["plain"], r["closure"]
+    # bulk-kernel roofline of the two lattices (fresh runs, 10 launches each)
+    bulk = {}
+    cp = closure.coarse_params(fine_p)
+    cp.storage = _lib.STORAGE_F16
+    for name, p, s_f in (("fine_f32", fine_p, 4), ("coarse_f16", cp, 2)):
         sim = Simulation(p)
-        keep = None
-        if net is not None and name == "f16_closure":
-            n = sim.cells
-            nut = torch.zeros(n, device=sim.device)
-            cs = torch.ones(n, device=sim.device)
-            out = torch.empty(n, 2, device=sim.device)
-            feats = torch.empty(n, _lib.MLP_IN, device=sim.device)
-            cl = _lib.Closure(nut.data_ptr(), cs.data_ptr())
-            sim.p.closure = ct.addressof(cl)
-            keep = (nut, cs, out, feats, cl)
         sim.init()
-        sim.step(2, store_macros=True)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(sim.torch_stream)
-        i = 0
-        while i < steps:
-            j = min(update_every, steps - i)
-            if keep is not None:
-                nut, cs, out, feats, _ = keep
-                _lib.check(L.ssmd_closure_features(ct.byref(sim.p), ct.byref(sim.fields), feats.data_ptr(),
-                                                   sim.stream))
-                _lib.check(L.ssmd_closure_apply(ct.byref(sim.p), net.net.data_ptr(), feats.data_ptr(),
-                                                out.data_ptr(), nut.data_ptr(), cs.data_ptr(), 0.05, sim.stream))
-            sim.step(j, store_macros=True)
-            i += j
-        e1.record(sim.torch_stream)
-        e1.synchronize()
-        dt = e0.elapsed_time(e1) / 1e3
+        sim.step(2)
         bm = bulk_launch_ms(sim, 10)
-        s_f = 4 if stg == _lib.STORAGE_F32 else 2
-        stats[name] = jet_stats(sim)
-        res[name] = {"mlups": round(sim.cells * steps / dt / 1e6, 1), "ms_per_step": round(dt * 1e3 / steps, 3),
-                     "bulk_ms": round(bm, 3),
-                     "roofline_frac": round(b_alg(27, s_f) * sim.cells / (bm * 1e-3) / 1e9 / peak, 4),
-                     "device_gb": round(torch.cuda.max_memory_allocated(sim.device) / 1e9, 1),
-                     "status": sim.check_status()}
+        bulk[name] = {"bulk_ms": round(bm, 3),
+                      "roofline_frac": round(b_alg(27, s_f) * sim.cells / (bm * 1e-3) / 1e9 / peak, 4),
+                      "device_gb": round(torch.cuda.max_memory_allocated() / 1e9, 1)}
         sim.close()
-        del sim, keep
+        del sim
         torch.cuda.empty_cache()
         torch.cuda.reset_peak_memory_stats()
-    res["f16_closure_vs_f32_plain"] = stat_diffs(stats["f16_closure"], stats["f32_plain"])
-    res["time_ratio"] = round(res["f16_closure"]["ms_per_step"] / res["f32_plain"]["ms_per_step"], 4)
-    return res
-
-
-def run_closure(full: bool):
-    """Coarse-plus-closure run against the fine run it learns from (D3Q19 oil
-    jet, 2x coarsening).  Default (full): fine 256 x 256 x 1024 for 20000
-    steps, the size of the closure study's fine runs (one seed of its eight);
-    --closure-small: fine 128 x 128 x 512 for 4000 steps."""
-    from ssmdlbm_b200 import closure, configs
-    if full:
-        shape, steps, every, spin, train, diam = (256, 256, 1024), 20000, 1000, 10000, 4000, 32
-    else:
-        shape, steps, every, spin, train, diam = (128, 128, 512), 4000, 200, 2000, 2000, 16
-    fine = configs.oil_jet(*shape, 19, tau=0.55, sigma=1e-3, width=4.0, mobility=0.1, diam=diam, w_in=0.05,
-                           noise=0.01, seed=0)
-    r = closure.experiment(fine, steps=steps, sample_every=every, spinup=spin, train_steps=train, batch=65536,
-                           lr=1e-3, seed=0, update_every=10)
-    f, pl, cl = r["fine"], r["plain"], r["closure"]
+    net = r["net"]
+    mlups = lambda s: round(s.cells * s.steps / s.device_s / 1e6, 1)
+    keys = ("centreline_uz", "centreline_phi", "phi_volume", "droplets", "droplet_volume", "droplets_per_snapshot",
+            "droplet_hist_l1")
     return {
-        "workload": f"oil jet D3Q19+D3Q7 fine {shape[0]}x{shape[1]}x{shape[2]}, {steps} steps, nozzle {diam}, "
-                    f"tau 0.55, sigma 1e-3, M 0.1, w 0.05 + 1% noise; coarse 2x, {steps // 2} steps; "
-                    f"closure refreshed every 10 coarse steps",
-        "device_s": {"fine": round(f.device_s, 4), "coarse_plain": round(pl.device_s, 4),
-                     "coarse_closure": round(cl.device_s, 4), "training": round(r["train_device_s"], 4)},
-        "time_ratio_closure_vs_fine": round(cl.device_s / f.device_s, 4),
-        "errors_vs_fine": {k: {"plain": r["errors_plain"][k], "closure": r["errors_closure"][k]}
-                           for k in ("centreline_uz", "centreline_phi", "phi_volume", "droplets",
-                                     "droplet_volume")},
-        "heldout_loss": r["heldout_loss"], "samples": r["samples"], "mlp_status": r["mlp_status"],
-        "mlp": mlp_throughput(),
-    }, r["net"]
+        "workload": f"oil jet D3Q27+D3Q7 fine 384x384x1536 FP32 plain, {steps} steps, nozzle 24, w 0.06 + 1% noise, "
+                    f"seed 3, tau 0.52, sigma 1e-3; coarse 192x192x768 FP16 storage, {steps // 2} steps, "
+                    f"closure refreshed every {update_every} coarse steps; statistics averaged over steps "
+                    f"{spinup}..{steps} every {sample_every}",
+        "steps": steps,
+        "fine": {"mlups": mlups(f), "device_s": round(f.device_s, 3), **bulk["fine_f32"]},
+        "coarse_plain": {"mlups": mlups(pl), "device_s": round(pl.device_s, 3)},
+        "coarse_closure": {"mlups": mlups(cl), "device_s": round(cl.device_s, 3), **bulk["coarse_f16"]},
+        "training": {"device_s": round(r["train_device_s"], 3), "adam_steps": train_steps, "samples": r["samples"],
+                     "heldout_loss": r["heldout_loss"], "reproducible_gradient": True},
+        "time_ratio": round(cl.device_s / f.device_s, 4),
+        "time_ratio_plain_coarse": round(pl.device_s / f.device_s, 4),
+        "errors_vs_filtered_fine": {k: {"plain": r["errors_plain"][k], "closure": r["errors_closure"][k]}
+                                    for k in keys},
+        "fine_droplets_per_snapshot": f.droplets_mean,
+        "mlp_status": r["mlp_status"],
+        "mlp": mlp_throughput(net),
+    }
+
+
+def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000):
+    """The closure study's data generation and training: fine D3Q19 jets
+    256 x 256 x 1024 (nozzle 32, tau 0.55, sigma 1e-3, M 0.1, 1 % noise),
+    inlet w ~ U[0.04, 0.08] per seed, `steps` steps each, filtered 2x onto
+    128 x 128 x 512 every 1000 steps from step 10000 (the last snapshot of
+    each seed held out); one network trained on all seeds (Adam, lr 1e-3,
+    batch 65536, `train_steps` steps, reproducible gradient); per seed, the
+    held-out loss and the coarse run with and without the closure against
+    the filtered fine run."""
+    import numpy as np
+    import torch
+    from ssmdlbm_b200 import closure, configs
+    rng = np.random.default_rng(4)
+    ws = rng.uniform(0.04, 0.08, seeds)
+    data = closure.Dataset()
+    fines, held = [], []
+    for i, w in enumerate(ws):
+        p = configs.oil_jet(256, 256, 1024, 19, tau=0.55, sigma=1e-3, width=4.0, mobility=0.1, diam=32,
+                            w_in=float(w), noise=0.01, seed=100 + i)
+        d = closure.Dataset()
+        fines.append((p, closure.fine_run(p, steps, 1000, 10000, 0.05, d)))
+        f, t, wt = d.cat()
+        nc = d.feats[-1].shape[0]
+        held.append((f[-nc:], t[-nc:], wt[-nc:]))
+        data.feats.append(f[:-nc])
+        data.targets.append(t[:-nc])
+        data.weights.append(wt[:-nc])
+        del d
+    feats, tg, wt = data.cat()
+    net = closure.Network(0)
+    net.normalise(feats, tg)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    curve = net.train(feats, tg, wt, train_steps, 65536, 1e-3, 0, report_every=max(1, train_steps // 10))
+    e1.record()
+    e1.synchronize()
+    per_seed = []
+    for (p, fine), (hf, ht, hw), w in zip(fines, held, ws):
+        base = closure.Network(0)
+        base.net.copy_(net.net)
+        P, I, O = 5378, 12, 2
+        base.net[:P] = 0.0
+        base.net[P + 2 * I + O:] = torch.tensor([0.0, 1.0], device=base.device)  # nu_t = 0, factor 1
+        cp = closure.coarse_params(p)
+        plain = closure.coarse_run(cp, steps // 2, 500, 5000, None, nut_max=0.05)
+        closed = closure.coarse_run(cp, steps // 2, 500, 5000, net, 10, 0.05)
+        per_seed.append({"w_in": round(float(w), 4),
+                         "heldout_loss": {"no_closure": base.loss_on(hf, ht, hw), "trained": net.loss_on(hf, ht, hw)},
+                         "errors_plain": closure.stat_errors(plain, fine),
+                         "errors_closure": closure.stat_errors(closed, fine),
+                         "fine_droplets_per_snapshot": fine.droplets_mean,
+                         "time_ratio_closure": round(closed.device_s / fine.device_s, 4)})
+    return {"workload": f"C4: {seeds} fine D3Q19 jets 256x256x1024, {steps} steps, w ~ U[0.04, 0.08]; "
+                        f"one network, {train_steps} Adam steps at batch 65536", "samples": int(feats.shape[0]),
+            "train_device_s": round(e0.elapsed_time(e1) / 1e3, 3), "train_curve": curve, "seeds": per_seed}
 
 
 def run_ours(a, world, rank, local):
@@ -569,8 +656,8 @@ def run_ours(a, world, rank, local):
 
     # live roofline of the dominant kernel
     bulk_ms = bulk_launch_ms(sim, 40)
-    s_f0 = 4 if a.storage == "f32" else 2
-    bytes_per_launch = b_alg(a.vs, s_f0) * sim.cells
+    s_f0, s_g0 = element_sizes(STORAGE_NAMES[a.storage])
+    bytes_per_launch = b_alg(a.vs, s_f0, s_g0) * sim.cells
     peak, peak_kind = hbm_peak()
     achieved = bytes_per_launch / (bulk_ms * 1e-3) / 1e9
     n_bc = 1  # oil inflow + outflow z in one launch (x, y exact periodic: no ghost copies)
@@ -586,6 +673,7 @@ def run_ours(a, world, rank, local):
     variants = {}
     if extras:
         for name, q, stg in (("d3q27_f16", 27, _lib.STORAGE_F16), ("d3q27_bf16", 27, _lib.STORAGE_BF16),
+                             ("d3q27_f16_g32", 27, _lib.STORAGE_F16_G32),
                              ("d3q19_f32", 19, _lib.STORAGE_F32), ("d3q19_f16", 19, _lib.STORAGE_F16)):
             pv = workload(stg, q)
             sv = Simulation(pv)
@@ -593,19 +681,18 @@ def run_ours(a, world, rank, local):
             sv.init()
             dv = time_graph(sv, a.steps, a.warmup, world)
             bm = bulk_launch_ms(sv, 20)
-            s_f = 4 if stg == _lib.STORAGE_F32 else 2
+            s_f, s_g = element_sizes(stg)
             variants[name] = {"mlups": round(sv.cells * a.steps / dv / 1e6, 1),
                               "bulk_path": int(sv.p.bulk_path), "tile_z": int(sv.p.tile_z),
-                              "bulk_ms": round(bm, 4),
-                              "roofline_frac": round(b_alg(q, s_f) * sv.cells / (bm * 1e-3) / 1e9 / peak, 4)}
+                              "bulk_ms": round(bm, 4), "bytes_per_cell": b_alg(q, s_f, s_g),
+                              "roofline_frac": round(b_alg(q, s_f, s_g) * sv.cells / (bm * 1e-3) / 1e9 / peak, 4)}
             sv.close()
             del sv
             torch.cuda.empty_cache()
 
     sweep = run_sweep() if extras else None
-    closure_line, net = run_closure(not a.closure_small) if (extras and not a.no_closure) else (None, None)
     precision = run_precision() if extras else None
-    production = run_production(net) if (extras and not a.no_production) else None
+    production = run_production() if (extras and not a.no_production) else None
 
     p.bulk_path, p.tile_z = sim_path, sim_tz
     e2e_steps = max(20, a.steps)  # the headline's job: K steps from the host's initial state
@@ -636,14 +723,13 @@ def run_ours(a, world, rank, local):
                      "traffic": (int(NCU_BYTES_PER_CELL[(a.vs, a.storage)] * NX * NY * NZ)
                                  if (a.vs, a.storage) in NCU_BYTES_PER_CELL and not a.size else None),
                      "peak_kind": peak_kind, "kernel": f"ssmd::bulk_kernel<{a.vs},{a.storage}>",
-                     "bytes_per_cell": b_alg(a.vs, s_f0), "launch_ms": round(bulk_ms, 4)},
+                     "bytes_per_cell": b_alg(a.vs, s_f0, s_g0), "launch_ms": round(bulk_ms, 4)},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": a.steps * (1 + n_bc),
         "clocks": clocks,
         "variants": variants,
         "sweep": sweep,
-        "closure": closure_line,
         "precision": precision,
         "production": production,
         "stats": {"u_max": st["u_max"], "phi_sum": st["phi_sum_next"], "status": st["status"]},
@@ -664,10 +750,25 @@ def run_reference(a, world, rank):
     # the reference cannot express inlet noise, the centred nozzle, exact periodic
     # faces or M = 0.1; its closest run: same lattice, velocity sets, tau, sigma,
     # nozzle diameter and inlet speed, its own boundary set with y copy-periodic.
-    out = subprocess.run([exe, "--periodic-y", "--time", f"{a.warmup},{a.steps}"], capture_output=True,
-                         text=True, timeout=1200, check=True).stdout
-    r = json.loads(out.strip().splitlines()[-1])
+    def timed(case):
+        out = subprocess.run([obuild.ref_binary(case), "--periodic-y", "--time", f"{a.warmup},{a.steps}"],
+                             capture_output=True, text=True, timeout=1200, check=True).stdout
+        return json.loads(out.strip().splitlines()[-1])
+
+    r = timed("q27_c2")
     v = r["mlups"]
+    # the reference's other builds of the same lattice: D3Q19 with FP32
+    # populations, and D3Q27 with ENABLE_FP16=1 (its default build, compile.sh:69:
+    # f - w as __half, g as float, src/cuda/utils.cuh:67-99)
+    variants = {}
+    for name, case, s_f, s_g in (("d3q19_f32", "q19_c2", 4, 4), ("d3q27_f16", "q27_c2_h", 2, 4)):
+        if not os.path.exists(obuild.ref_binary(case)):
+            variants[name] = {"unavailable": f"reference harness {case} not built"}
+            continue
+        rv = timed(case)
+        variants[name] = {"mlups": round(rv["mlups"], 1), "ms_per_step": rv["ms_per_step"],
+                          "build": f"D3Q{rv['Q']}, ENABLE_FP16={rv['fp16']}",
+                          "population_bytes_per_cell": 2 * (rv["Q"] * s_f + 7 * s_g)}
     return {
         "metric": "MLUPS", "value": round(v, 1), "unit": "MLUPS", "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -682,6 +783,7 @@ def run_reference(a, world, rank):
                                    "path), built for sm_100a from its sources, driven by one host "
                                    "thread with its per-step stream synchronisation"},
         "e2e": {"value": round(v, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_variants": variants,
     }
 
 
@@ -692,17 +794,14 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quick", action="store_true",
-                    help="headline only: skip the variants, sweep, closure, precision and production legs")
+                    help="headline only: skip the variants, sweep, precision and production legs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", default=None, help="nx,ny,nz of a smaller lattice (profiling runs)")
     ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
-    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
-    ap.add_argument("--no-production", action="store_true",
-                    help="skip the 384 x 384 x 1536 production-lattice leg")
-    ap.add_argument("--closure-small", action="store_true",
-                    help="closure leg at 128 x 128 x 512, 4000 steps (seconds) instead of 256 x 256 x 1024, 20000 steps")
+    ap.add_argument("--c4", action="store_true",
+                    help="run only the closure study's data generation and training (8 fine seeds, about 12 min)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                     help="bulk kernel path: 0 auto, 1 gathers, 2 TMA phi boxes, 3 TMA population slabs")
     a = ap.parse_args()
@@ -711,7 +810,9 @@ def main() -> int:
         NX, NY, NZ = (int(v) for v in a.size.split(","))
     a.warmup = max(a.warmup, 3)  # at least 3 untimed steps
     world, rank, local = dist_setup(a.gpus)
-    if a.impl == "reference":
+    if a.c4:
+        line = {"metric": "closure study (C4)", **run_c4()} if rank == 0 else None
+    elif a.impl == "reference":
         line = run_reference(a, world, rank)
     else:
         line = run_ours(a, world, rank, local)

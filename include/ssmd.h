@@ -66,6 +66,10 @@ typedef struct CUgraphExec_st *ssmd_graph_exec_t;
 #define SSMD_STORAGE_BF16 2 /* f - w_q as bfloat16, g as IEEE half (both round
                                to nearest; g carries phi in [0, 1], which
                                needs mantissa bits rather than range)     */
+#define SSMD_STORAGE_F16_G32 3 /* f - w_q as IEEE half, g as float: the layout
+                                  of the reference's ENABLE_FP16=1 build
+                                  (src/cuda/utils.cuh:67-99, pop_t f and
+                                  scalar_t g in src/structs/LBMFields.cuh) */
 
 /* ------------------------------------------------- bulk kernel variants */
 #define SSMD_PATH_AUTO 0   /* library choice (currently SSMD_PATH_GATHER)        */
@@ -123,7 +127,8 @@ typedef struct LBMFields {
     float *fsy;
     float *fsz;
     void *f; /* Q * cells populations, element type from ssmd_params.storage */
-    void *g; /* 7 * cells phase populations, same element type              */
+    void *g; /* 7 * cells phase populations: float for SSMD_STORAGE_F32 and
+                SSMD_STORAGE_F16_G32, IEEE half otherwise                */
 } LBMFields;
 
 /*
@@ -444,11 +449,18 @@ int ssmd_derived_update(const ssmd_params *p, const LBMFields *fields, uint32_t 
 
 /*
  * Learned closure (no reference counterpart).  The network runs on the
- * tcgen05 tensor cores, 128 cells per CTA, bf16 operands, FP32 accumulation.
- *   ssmd_mlp_forward: out[i][0..1] = scale * net(features[i]) + offset.
+ * tcgen05 tensor cores, 128 cells per CTA, bf16 operands, FP32 accumulation,
+ * GELU in its tanh form z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
+ *   ssmd_mlp_forward: out[i][0..1] = scale * net(features[i]) + offset
+ *     (out 8-byte aligned).
  *   ssmd_mlp_grad: overwrites grad (SSMD_MLP_PARAMS floats) with dL/dparams
  *     and *loss (device double) with L = (1/n) sum_i sum_k w_ik (r_ik -
  *     (t_ik - offset_k)/scale_k)^2, r the raw output; weights may be NULL (1).
+ *     The CTAs' sums meet in floating-point atomics, so the last bits vary
+ *     from run to run.
+ *   ssmd_mlp_grad_ws: the same, reproducible bit for bit: every CTA writes its
+ *     sums to a row of `workspace` (ssmd_mlp_grad_workspace_bytes() bytes,
+ *     device memory) and a second kernel adds the rows in CTA order.
  *   ssmd_mlp_adam: one Adam step (bias-corrected, step t >= 1) on the params.
  *   ssmd_mlp_status: bit 0 set when an MMA wait timed out (the CTA aborted).
  * Features (ssmd_closure_features), per cell, from rho, ux, uy, uz, phi with
@@ -468,10 +480,17 @@ int ssmd_derived_update(const ssmd_params *p, const LBMFields *fields, uint32_t 
  * network on features and writes nut = clamp(out0, max(-nu(phi)/2, -nut_max),
  * nut_max) (nu(phi) is feature 11) and
  * sigma_scale = clamp(out1, 0.25, 4); out is 2 * cells floats of scratch.
+ * ssmd_closure_refresh does features, network and apply in one kernel (the
+ * features never leave the chip): the same nut and sigma_scale as
+ * ssmd_closure_features + ssmd_closure_apply, without their buffers.
  */
 int ssmd_mlp_forward(const float *net, const float *features, int64_t n, float *out, ssmd_stream_t stream);
 int ssmd_mlp_grad(const float *net, const float *features, const float *targets, const float *weights, int64_t n,
                   float *grad, double *loss, ssmd_stream_t stream);
+size_t ssmd_mlp_grad_workspace_bytes(void);
+int ssmd_mlp_grad_ws(const float *net, const float *features, const float *targets, const float *weights,
+                     int64_t n, float *grad, double *loss, float *workspace, size_t workspace_bytes,
+                     ssmd_stream_t stream);
 int ssmd_mlp_adam(float *net, const float *grad, float *m, float *v, int64_t t, float lr, float beta1,
                   float beta2, float eps, ssmd_stream_t stream);
 int ssmd_mlp_status(uint32_t *status);
@@ -482,6 +501,8 @@ int ssmd_closure_targets(const ssmd_params *coarse, const float *coarse_fields, 
                          const float *area, float nut_max, float *targets, float *weights, ssmd_stream_t stream);
 int ssmd_closure_apply(const ssmd_params *coarse, const float *net, const float *features, float *out,
                        float *nut, float *sigma_scale, float nut_max, ssmd_stream_t stream);
+int ssmd_closure_refresh(const ssmd_params *coarse, const LBMFields *fields, const float *net, float nut_max,
+                         float *nut, float *sigma_scale, ssmd_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,9 @@
 * oracle/_build/libssmd_oracle.so — ssmd_oracle.cpp, g++ -O2 -fopenmp
   -ffp-contract=off (no FMA contraction, so the FP32 instantiation follows
   the written operation order).
+* oracle/_build/libssmd_oracle_gpu.so — ssmd_oracle_gpu.cu, the same
+  per-cell functions (oracle_cells.h) as FP64 CUDA kernels, nvcc for sm_100a
+  with --fmad=false (no contraction, so it matches the CPU build bit for bit).
 * oracle/_ref/<case>/harness — the reference's own kernels, compiled by nvcc
   for sm_100a from the reference's sources where they lie (REF_SRC), with
   oracle/ref_harness/constants.cuh.in filled in per case and placed first on
@@ -34,6 +37,7 @@ ROOT = os.path.dirname(HERE)
 REF_ROOT = os.environ.get("SSMD_REFERENCE", "/root/reference")
 REF_SRC = os.path.join(REF_ROOT, "src")
 ORACLE_SO = os.path.join(HERE, "_build", "libssmd_oracle.so")
+ORACLE_GPU_SO = os.path.join(HERE, "_build", "libssmd_oracle_gpu.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 # Reference-expressible cases.  diam/radius/Re/We are the reference's own
@@ -59,10 +63,30 @@ CASES = {
 }
 
 
+def _oracle_deps(src: str) -> list[str]:
+    return [src, os.path.join(HERE, "oracle_cells.h"), os.path.join(ROOT, "include", "ssmd.h"),
+            os.path.join(ROOT, "ssmdlbm_b200", "csrc", "noise.h")]
+
+
+def build_oracle_gpu(force: bool = False) -> str:
+    src = os.path.join(HERE, "ssmd_oracle_gpu.cu")
+    deps = _oracle_deps(src)
+    if not force and os.path.exists(ORACLE_GPU_SO) and all(
+            os.path.getmtime(d) <= os.path.getmtime(ORACLE_GPU_SO) for d in deps):
+        return ORACLE_GPU_SO
+    os.makedirs(os.path.dirname(ORACLE_GPU_SO), exist_ok=True)
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cmd = [nvcc, "-O3", "--fmad=false", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-Xcompiler", "-fPIC", "-shared", "-cudart", "static", src, "-o", ORACLE_GPU_SO]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"GPU oracle build failed:\n{r.stdout}\n{r.stderr}")
+    return ORACLE_GPU_SO
+
+
 def build_oracle(force: bool = False) -> str:
     src = os.path.join(HERE, "ssmd_oracle.cpp")
-    deps = [src, os.path.join(ROOT, "include", "ssmd.h"),
-            os.path.join(ROOT, "ssmdlbm_b200", "csrc", "noise.h")]
+    deps = _oracle_deps(src)
     if not force and os.path.exists(ORACLE_SO) and all(
             os.path.getmtime(d) <= os.path.getmtime(ORACLE_SO) for d in deps):
         return ORACLE_SO
@@ -160,6 +184,7 @@ if __name__ == "__main__":
     both = not (a.oracle or a.ref)
     if a.oracle or both:
         print(build_oracle(a.force))
+        print(build_oracle_gpu(a.force))
     if a.ref or both:
         for e in build_ref(a.force):
             print(e)

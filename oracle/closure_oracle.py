@@ -5,9 +5,13 @@ reference counterpart (the reference runs the plain method only); this file
 states what ssmdlbm_b200/csrc/mlp.cu and closure.cu compute so that their
 results can be checked:
 
-- the network 12 -> 64 -> 64 -> 2 with GELU (erf form), in FP64 apart from
-  the bf16 rounding of every tensor-core operand (standardised features,
-  weights, hidden activations, dZ2), which is emulated bit for bit;
+- the network 12 -> 64 -> 64 -> 2 with GELU in its tanh form
+  (z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), Hendrycks & Gimpel 2016),
+  in FP64 apart from the bf16 rounding of every tensor-core operand
+  (standardised features, weights, hidden activations, dZ2), which is
+  emulated; the kernel's tanh is the SFU's tanh.approx.f32 (absolute error
+  about 2^-11), so an activation near a bf16 rounding boundary may round the
+  other way there;
 - its loss and gradient (the backward pass written out by hand) and Adam;
 - features, 2x box filter and training targets, in FP32 arithmetic on
   [z][y][x] numpy arrays.
@@ -15,7 +19,6 @@ results can be checked:
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 IN, HID, OUT, K1 = 12, 64, 2, 16
 oW1 = 0
@@ -40,12 +43,17 @@ def bf16(x) -> np.ndarray:
     return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32).reshape(a.shape)
 
 
+G0 = np.sqrt(2.0 / np.pi)
+G1 = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(G0 * (z + G1 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(G0 * (z + G1 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * G0 * (1.0 + 3.0 * G1 * z * z)
 
 
 def unpack(net):

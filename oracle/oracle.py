@@ -1,7 +1,8 @@
-"""Python handle on the CPU oracle (libssmd_oracle.so).  TEST INFRASTRUCTURE.
+"""Python handles on the oracle: the CPU build (libssmd_oracle.so) and its
+FP64 GPU instance (libssmd_oracle_gpu.so).  TEST INFRASTRUCTURE.
 
-Only tests, the smoke check and bench.py's CPU-baseline leg use this module;
-the product path (ssmdlbm_b200) never imports it.
+Only tests, fixture scripts, the smoke check and bench.py's CPU-baseline leg
+use this module; the product path (ssmdlbm_b200) never imports it.
 
 Arrays are numpy, scalar fields shaped [z][y][x], populations [q][z][y][x] in
 the reference's push layout.
@@ -39,6 +40,10 @@ def lib():
         L.oracle_centreline.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_droplets.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.oracle_centreline_arrays.argtypes = [ctypes.c_void_p] * 5
+        L.oracle_droplets_arrays.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_void_p]
         L.oracle_noise.restype = ctypes.c_double
         L.oracle_noise.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
         _lib = L
@@ -100,17 +105,107 @@ class Oracle:
 
     def droplets(self, threshold: float = 0.5, max_droplets: int = 100000):
         """Components as a structured array (root, cells, volume, touches_inlet), sorted by root."""
-        root = np.zeros(max_droplets, np.uint32)
-        cells = np.zeros(max_droplets, np.uint32)
-        vol = np.zeros(max_droplets, np.float64)
-        touch = np.zeros(max_droplets, np.uint32)
-        n = ctypes.c_int()
-        lib().oracle_droplets(self.h, threshold, root.ctypes.data, cells.ctypes.data, vol.ctypes.data,
-                              touch.ctypes.data, max_droplets, ctypes.byref(n))
-        k = min(n.value, max_droplets)
-        out = np.zeros(k, dtype=[("root", "u4"), ("cells", "u4"), ("volume", "f8"), ("touches_inlet", "u4")])
-        out["root"], out["cells"], out["volume"], out["touches_inlet"] = root[:k], cells[:k], vol[:k], touch[:k]
-        return out
+        return _droplets(lambda *a: lib().oracle_droplets(self.h, threshold, *a), max_droplets)
+
+
+def _droplets(call, max_droplets: int):
+    root = np.zeros(max_droplets, np.uint32)
+    cells = np.zeros(max_droplets, np.uint32)
+    vol = np.zeros(max_droplets, np.float64)
+    touch = np.zeros(max_droplets, np.uint32)
+    n = ctypes.c_int()
+    call(root.ctypes.data, cells.ctypes.data, vol.ctypes.data, touch.ctypes.data, max_droplets, ctypes.byref(n))
+    k = min(n.value, max_droplets)
+    out = np.zeros(k, dtype=[("root", "u4"), ("cells", "u4"), ("volume", "f8"), ("touches_inlet", "u4")])
+    out["root"], out["cells"], out["volume"], out["touches_inlet"] = root[:k], cells[:k], vol[:k], touch[:k]
+    return out
+
+
+_gpu_lib = None
+
+
+def gpu_lib():
+    global _gpu_lib
+    if _gpu_lib is None:
+        path = _build.ORACLE_GPU_SO
+        if not os.path.exists(path):
+            path = _build.build_oracle_gpu()
+        L = ctypes.CDLL(path)
+        L.oracle_gpu_new.restype = ctypes.c_void_p
+        L.oracle_gpu_new.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_gpu_free.argtypes = [ctypes.c_void_p]
+        L.oracle_gpu_init_jets.argtypes = [ctypes.c_void_p]
+        L.oracle_gpu_init_macros.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
+        L.oracle_gpu_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_gpu_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.oracle_gpu_last_error.restype = ctypes.c_char_p
+        _gpu_lib = L
+    return _gpu_lib
+
+
+class GpuOracle:
+    """The oracle on the current CUDA device (same interface as Oracle):
+    precision 64 (FP64 transcription) or 32 (the reference's FP32
+    arithmetic), bit-identical to the CPU build of the same precision.  It
+    allocates its own device memory: Q + 25 reals per cell (+ 7 with
+    omega_g != 1)."""
+
+    def __init__(self, params, precision: int = 64):
+        self.p = params
+        self.precision = precision
+        self.h = gpu_lib().oracle_gpu_new(ctypes.byref(params), precision)
+        if not self.h:
+            raise RuntimeError("oracle_gpu_new failed: " + gpu_lib().oracle_gpu_last_error().decode())
+        self.Q = int(params.velocity_set)
+        self.shape = (int(params.nz), int(params.ny), int(params.nx))
+        self.cells = int(np.prod(self.shape))
+        self.steps_done = 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            gpu_lib().oracle_gpu_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise RuntimeError(gpu_lib().oracle_gpu_last_error().decode())
+
+    def init_jets(self) -> None:
+        self._check(gpu_lib().oracle_gpu_init_jets(self.h))
+        self.steps_done = 0
+
+    def init_macros(self, rho, ux, uy, uz, phi) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32).reshape(-1) for a in (rho, ux, uy, uz, phi)]
+        self._check(gpu_lib().oracle_gpu_init_macros(self.h, *[a.ctypes.data for a in arrs]))
+        self.steps_done = 0
+
+    def step(self, n: int = 1) -> None:
+        self._check(gpu_lib().oracle_gpu_step(self.h, n))
+        self.steps_done += n
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.cells * (self.Q if name == "f" else 7 if name == "g" else 1)
+        out = np.empty(n, dtype=np.float64)
+        self._check(gpu_lib().oracle_gpu_get(self.h, FIELD_IDS[name], out.ctypes.data))
+        if name in ("f", "g"):
+            return out.reshape((-1,) + self.shape)
+        return out.reshape(self.shape)
+
+    def centreline(self):
+        uz = np.zeros(self.shape[0])
+        phi = np.zeros(self.shape[0])
+        u, ph = self.get("uz"), self.get("phi")
+        lib().oracle_centreline_arrays(ctypes.byref(self.p), u.ctypes.data, ph.ctypes.data, uz.ctypes.data,
+                                       phi.ctypes.data)
+        return uz, phi
+
+    def droplets(self, threshold: float = 0.5, max_droplets: int = 100000):
+        ph = self.get("phi")
+        return _droplets(lambda *a: lib().oracle_droplets_arrays(ctypes.byref(self.p), ph.ctypes.data, threshold,
+                                                                 *a), max_droplets)
 
 
 def noise(seed: int, step: int, cell: int, stream: int = 0) -> float:

@@ -27,6 +27,7 @@ BC_JET = 2
 STORAGE_F32 = 0
 STORAGE_F16 = 1
 STORAGE_BF16 = 2
+STORAGE_F16_G32 = 3  # f - w as half, g as float: the reference's ENABLE_FP16=1 layout
 
 STEP_STORE_MACROS = 1
 STEP_AVERAGE = 2
@@ -163,6 +164,9 @@ SIGNATURES = [
     ("ssmd_mlp_forward", c_int32, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
     ("ssmd_mlp_grad", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,
                                 c_void_p]),
+    ("ssmd_mlp_grad_workspace_bytes", ctypes.c_size_t, []),
+    ("ssmd_mlp_grad_ws", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p,
+                                   c_void_p, ctypes.c_size_t, c_void_p]),
     ("ssmd_mlp_adam", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_float, c_float,
                                 c_float, c_float, c_void_p]),
     ("ssmd_mlp_status", c_int32, [POINTER(c_uint32)]),
@@ -173,6 +177,8 @@ SIGNATURES = [
                                        c_void_p, c_void_p]),
     ("ssmd_closure_apply", c_int32, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_float, c_void_p]),
+    ("ssmd_closure_refresh", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_float, c_void_p, c_void_p,
+                                       c_void_p]),
 ]
 
 

@@ -52,9 +52,12 @@ def _save(d: dict) -> None:
 
 def candidates(p):
     paths = [_lib.PATH_GATHER]
-    esize = 4 if p.storage == _lib.STORAGE_F32 else 2
-    if (int(p.nx) * esize) % 16 == 0:
-        paths += [_lib.PATH_TMA, _lib.PATH_SLAB]
+    f_size = 4 if p.storage == _lib.STORAGE_F32 else 2
+    g_size = 4 if p.storage in (_lib.STORAGE_F32, _lib.STORAGE_F16_G32) else 2
+    if (int(p.nx) * g_size) % 16 == 0:
+        paths.append(_lib.PATH_TMA)  # TMA boxes of g
+    if f_size == g_size and (int(p.nx) * f_size) % 16 == 0:
+        paths.append(_lib.PATH_SLAB)  # f and g slabs of one element size
     nzf = int(p.nz) - (0 if p.bc_z == _lib.BC_PERIODIC else 2)
     return [(path, tz) for path in paths for tz in CANDIDATE_TILE_Z if tz == 0 or tz <= nzf]
 

@@ -90,7 +90,14 @@ class Network:
         self.v = torch.zeros(_lib.MLP_PARAMS, device=self.device)
         self.grad = torch.zeros(_lib.MLP_PARAMS, device=self.device)
         self.loss = torch.zeros(1, dtype=torch.float64, device=self.device)
+        # per-CTA gradient rows of ssmd_mlp_grad_ws: the same bits on every run
+        self.ws = torch.empty(lib().ssmd_mlp_grad_workspace_bytes() // 4, device=self.device)
         self.t = 0
+
+    def _grad(self, feats, targets, weights, n, stream) -> None:
+        check(lib().ssmd_mlp_grad_ws(self.net.data_ptr(), feats.data_ptr(), targets.data_ptr(),
+                                     weights.data_ptr() if weights is not None else None, n, self.grad.data_ptr(),
+                                     self.loss.data_ptr(), self.ws.data_ptr(), self.ws.numel() * 4, stream))
 
     def normalise(self, feats: torch.Tensor, targets: torch.Tensor) -> None:
         """Feature standardisation and output scaling from training data."""
@@ -106,10 +113,7 @@ class Network:
 
     def loss_on(self, feats, targets, weights=None) -> float:
         """Weighted mean squared error in normalised output units."""
-        n = feats.shape[0]
-        check(lib().ssmd_mlp_grad(self.net.data_ptr(), feats.data_ptr(), targets.data_ptr(),
-                                  weights.data_ptr() if weights is not None else None, n, self.grad.data_ptr(),
-                                  self.loss.data_ptr(), torch.cuda.current_stream(self.device).cuda_stream))
+        self._grad(feats, targets, weights, feats.shape[0], torch.cuda.current_stream(self.device).cuda_stream)
         return float(self.loss.item())
 
     def train(self, feats, targets, weights, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0,
@@ -130,8 +134,7 @@ class Network:
             torch.index_select(feats, 0, idx, out=fb)
             torch.index_select(targets, 0, idx, out=tb)
             torch.index_select(weights, 0, idx, out=wb)
-            check(L.ssmd_mlp_grad(self.net.data_ptr(), fb.data_ptr(), tb.data_ptr(), wb.data_ptr(), b,
-                                  self.grad.data_ptr(), self.loss.data_ptr(), st))
+            self._grad(fb, tb, wb, b, st)
             self.t += 1
             check(L.ssmd_mlp_adam(self.net.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(), self.v.data_ptr(),
                                   self.t, lr, 0.9, 0.999, 1e-8, st))
@@ -161,17 +164,26 @@ class Dataset:
         return torch.cat(self.feats), torch.cat(self.targets), torch.cat(self.weights)
 
 
+# droplet-size histogram: detached component volume (sum of phi, fine-cell
+# units) in powers-of-two bins
+DROP_EDGES = np.concatenate([[0.0], 2.0 ** np.arange(0, 31)])
+
+
 @dataclass
 class JetStats:
-    """Statistics of one run, on the coarse lattice's z planes."""
+    """Statistics of one run, on the coarse lattice's z planes.  The
+    centreline profiles and the droplet counts are means over the sampled
+    snapshots; the histogram counts every detached droplet of every snapshot."""
     centreline_uz: np.ndarray
     centreline_phi: np.ndarray
     droplets: int
-    droplet_volume: float  # detached phi volume in fine-cell units
+    droplet_volume: float  # detached phi volume in fine-cell units (last snapshot)
     phi_volume: float      # total phi in fine-cell units
     device_s: float
     steps: int
     cells: int
+    droplets_mean: float = 0.0       # detached droplets per snapshot
+    droplet_hist: np.ndarray = None  # counts over DROP_EDGES, all snapshots
 
 
 def _view(coarse: torch.Tensor, nc: int) -> LBMFields:
@@ -205,6 +217,11 @@ def _stats_snapshot(sim, acc: dict, cp: Params | None = None) -> None:
     acc["uz"] = acc.get("uz", 0) + uz
     acc["phi"] = acc.get("phi", 0) + phi
     acc["n"] = acc.get("n", 0) + 1
+    d = sim.droplets(0.5)
+    vol_unit = 1.0 if cp is not None else 8.0  # coarse cells hold 8 fine cells
+    vols = d[d["touches_inlet"] == 0]["volume"].astype(np.float64) * vol_unit
+    acc["hist"] = acc.get("hist", 0) + np.histogram(vols, bins=DROP_EDGES)[0]
+    acc["ndrops"] = acc.get("ndrops", 0) + len(vols)
 
 
 def _finish(sim, acc: dict, fine: bool, device_s: float, steps: int) -> JetStats:
@@ -218,7 +235,8 @@ def _finish(sim, acc: dict, fine: bool, device_s: float, steps: int) -> JetStats
     detached = d[d["touches_inlet"] == 0]
     total = float(sim.field("phi").astype(np.float64).sum()) * vol_unit
     return JetStats(uz, phi, int(len(detached)), float(detached["volume"].sum()) * vol_unit, total, device_s,
-                    steps, sim.cells)
+                    steps, sim.cells, droplets_mean=acc["ndrops"] / acc["n"],
+                    droplet_hist=np.asarray(acc["hist"], np.int64))
 
 
 def fine_run(p: Params, steps: int, sample_every: int, spinup: int, nut_max: float = 0.05,
@@ -278,7 +296,8 @@ def _timed_steps(sim, k: int) -> float:
 def coarse_run(cp: Params, steps: int, sample_every: int, spinup: int, net: Network | None = None,
                update_every: int = 1, nut_max: float = 0.05) -> JetStats:
     """The coarse lattice, plain (net None) or with the closure refreshed every
-    `update_every` steps from the fields of the step before."""
+    `update_every` steps from the fields of the step before (features,
+    network and bounds in one kernel, ssmd_closure_refresh)."""
     from .lbm import Simulation
     L = lib()
     sim = Simulation(cp)
@@ -287,11 +306,9 @@ def coarse_run(cp: Params, steps: int, sample_every: int, spinup: int, net: Netw
         n = sim.cells
         nut = torch.zeros(n, device=sim.device)
         cs = torch.ones(n, device=sim.device)
-        out = torch.empty(n, 2, device=sim.device)
-        feats = torch.empty(n, _lib.MLP_IN, device=sim.device)
         cl = _lib.Closure(nut.data_ptr(), cs.data_ptr())
         sim.p.closure = ctypes.addressof(cl)
-        keep = (nut, cs, out, feats, cl)
+        keep = (nut, cs, cl)
     sim.init()
     acc: dict = {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -305,14 +322,13 @@ def coarse_run(cp: Params, steps: int, sample_every: int, spinup: int, net: Netw
         if net is None:
             sim.step(k, store_macros=True)
         else:
-            nut, cs, out, feats, _ = keep
+            nut, cs, _ = keep
             i = 0
             while i < k:
                 j = min(update_every, k - i)
                 # closure from the fields the previous step stored
-                check(L.ssmd_closure_features(ctypes.byref(sim.p), ctypes.byref(sim.fields), feats.data_ptr(), st))
-                check(L.ssmd_closure_apply(ctypes.byref(sim.p), net.net.data_ptr(), feats.data_ptr(),
-                                           out.data_ptr(), nut.data_ptr(), cs.data_ptr(), nut_max, st))
+                check(L.ssmd_closure_refresh(ctypes.byref(sim.p), ctypes.byref(sim.fields), net.net.data_ptr(),
+                                             nut_max, nut.data_ptr(), cs.data_ptr(), st))
                 sim.step(j, store_macros=True)
                 i += j
         e1.record(sim.torch_stream)
@@ -341,15 +357,20 @@ def stat_errors(s: JetStats, ref: JetStats) -> dict:
         "droplets": (s.droplets, ref.droplets),
         "droplet_volume": (abs(s.droplet_volume - ref.droplet_volume) / ref.droplet_volume
                            if ref.droplet_volume > 0 else None),
+        "droplets_per_snapshot": (s.droplets_mean, ref.droplets_mean),
+        # droplet-size histogram: L1 distance over the fine run's droplet count
+        "droplet_hist_l1": (float(np.abs(s.droplet_hist - ref.droplet_hist).sum()) / float(ref.droplet_hist.sum())
+                            if ref.droplet_hist is not None and ref.droplet_hist.sum() > 0 else None),
         "phi_volume": abs(s.phi_volume - ref.phi_volume) / max(ref.phi_volume, 1e-30),
     }
 
 
 def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train_steps: int = 2000,
                batch: int = 65536, lr: float = 1e-3, seed: int = 0, update_every: int = 1,
-               nut_max: float = 0.05) -> dict:
+               nut_max: float = 0.05, coarse_storage: int | None = None) -> dict:
     """Fine run (the judge and the data), training, then the coarse lattice
-    plain and with the trained closure; statistics, errors and device times."""
+    plain and with the trained closure (population storage `coarse_storage`,
+    default the fine run's); statistics, errors and device times."""
     data = Dataset()
     t0 = time.perf_counter()
     fine = fine_run(fine_p, steps, sample_every, spinup, nut_max, data)
@@ -379,6 +400,8 @@ def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train
     train_s = e0.elapsed_time(e1) / 1e3
     loss_after = net.loss_on(f_te, t_te, w_te)
     cp = coarse_params(fine_p)
+    if coarse_storage is not None:
+        cp.storage = coarse_storage
     csteps, cevery, cspin = steps // 2, max(1, sample_every // 2), spinup // 2
     plain = coarse_run(cp, csteps, cevery, cspin, None, nut_max=nut_max)
     closed = coarse_run(cp, csteps, cevery, cspin, net, update_every, nut_max)

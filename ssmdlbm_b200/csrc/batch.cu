@@ -144,7 +144,7 @@ int dispatch(int q, int storage, F &&f) {
     case 27 * 4 + SSMD_STORAGE_F32: return f(std::integral_constant<int, 27>{}, float{});
     case 27 * 4 + SSMD_STORAGE_F16: return f(std::integral_constant<int, 27>{}, __half{});
     case 27 * 4 + SSMD_STORAGE_BF16: return f(std::integral_constant<int, 27>{}, __nv_bfloat16{});
-    default: return fail(SSMD_ERR_UNSUPPORTED, "unsupported velocity set / storage");
+    default: return fail(SSMD_ERR_UNSUPPORTED, "unsupported velocity set / storage (batches: F32, F16, BF16)");
     }
 }
 

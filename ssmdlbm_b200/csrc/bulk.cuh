@@ -178,6 +178,7 @@ struct Bulk {
 
     static __device__ __forceinline__ float tofloat(float v) { return v; }
     static __device__ __forceinline__ float tofloat(__half v) { return __half2float(v); }
+    static __device__ __forceinline__ float tofloat(half_g32 v) { return __half2float(v.h); }
     static __device__ __forceinline__ float tofloat(__nv_bfloat16 v) { return __bfloat162float(v); }
 
     // Same as fill_phi, with the g values of fluid cells taken from the TMA

@@ -65,6 +65,20 @@ struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
+// Element type of the hydrodynamic populations under SSMD_STORAGE_F16_G32: an
+// IEEE half like __half, as its own type so that its lattice keeps the phase
+// populations in float (the reference's ENABLE_FP16=1 layout).
+struct __align__(2) half_g32 {
+    __half h;
+};
+template <>
+struct Store<half_g32> {
+    static __device__ __forceinline__ float ld(const half_g32 *p) { return __half2float(__ldg(&p->h)); }
+    static __device__ __forceinline__ float ldc(const half_g32 *p) { return __half2float(p->h); }
+    static __device__ __forceinline__ float ld_keep(const half_g32 *p) { return Store<__half>::ld_keep(&p->h); }
+    static __device__ __forceinline__ void st(half_g32 *p, float v) { p->h = __float2half_rn(v); }
+};
+
 // Phase-population (g) storage for a storage type: the same type, except that
 // BF16 runs keep g in IEEE half.  g carries phi in [0, 1], which needs mantissa
 // bits rather than exponent range; with BF16's 8 bits the small anti-diffusion
@@ -78,6 +92,10 @@ struct PhaseStore {
 template <>
 struct PhaseStore<__nv_bfloat16> {
     using type = __half;
+};
+template <>
+struct PhaseStore<half_g32> {
+    using type = float;
 };
 template <class T>
 using phase_t = typename PhaseStore<T>::type;

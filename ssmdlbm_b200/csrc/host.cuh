@@ -32,7 +32,9 @@ constexpr size_t kPartialOff = 512;
 constexpr int kMaxRedBlocks = 1024;
 constexpr size_t kWorkspaceBytes = kPartialOff + sizeof(double) * kRedVals * kMaxRedBlocks;
 
-inline size_t storage_size(int s) { return s == SSMD_STORAGE_F32 ? 4 : 2; }
+// element sizes of the hydrodynamic (f) and phase (g) populations
+inline size_t f_storage_size(int s) { return s == SSMD_STORAGE_F32 ? 4 : 2; }
+inline size_t g_storage_size(int s) { return (s == SSMD_STORAGE_F32 || s == SSMD_STORAGE_F16_G32) ? 4 : 2; }
 
 inline Geometry make_geometry(const ssmd_params &p) {
     Geometry G{};
@@ -278,14 +280,19 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     if (path == SSMD_PATH_TMA &&
         !encode_populations<TG>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, GBox<TG>::WX, kHY))
         return fail(SSMD_ERR_UNSUPPORTED, "TMA path needs nx * element size to be a multiple of 16 bytes");
+    // the slab path stages f and g slabs of one element size
+    constexpr bool kSlabs = sizeof(T) == sizeof(TG);
+    if (path == SSMD_PATH_SLAB && !kSlabs)
+        return fail(SSMD_ERR_UNSUPPORTED, "slab path needs f and g of one element size");
     if (path == SSMD_PATH_SLAB &&
         !(encode_populations<TG>(&gmap, a.g_src, a.geo.nx, a.geo.ny, a.geo.nz, 7, Slab<TG>::WX, kTY) &&
           encode_populations<T>(&fmap, a.f_src, a.geo.nx, a.geo.ny, a.geo.nz, Q, Slab<T>::WX, kTY)))
         return fail(SSMD_ERR_UNSUPPORTED, "slab path needs nx * element size to be a multiple of 16 bytes");
     int per_sm = 1, sms = 1;
     if (path == SSMD_PATH_TMA) bulk_slots<Q, T, 2>(per_sm, sms);
-    else if (path == SSMD_PATH_SLAB) bulk_slots<Q, T, 3>(per_sm, sms);
-    else bulk_slots<Q, T, 1>(per_sm, sms);
+    else if (path == SSMD_PATH_SLAB) {
+        if constexpr (kSlabs) bulk_slots<Q, T, 3>(per_sm, sms);
+    } else bulk_slots<Q, T, 1>(per_sm, sms);
     tiling(p, a.geo, per_sm * sms, a.tiles_x, a.tiles_y, a.zchunk, a.nzchunks);
     a.halo_mod = (a.geo.bcx == BC_PERIODIC && a.geo.nx < (uint32_t)(kTX + 4)) ||
                  (a.geo.bcy == BC_PERIODIC && a.geo.ny < (uint32_t)(kTY + 4)) ||
@@ -298,9 +305,9 @@ int launch_step(const ssmd_params &p, const LBMFields &fl, uint64_t step, uint32
     if (ev0) cudaEventRecord(ev0, st);
     if (path == SSMD_PATH_TMA)
         bulk_kernel<Q, T, TG, 2><<<nblk, blk, bulk_dyn_smem<Q, T, 2>(), st>>>(a, gmap, fmap);
-    else if (path == SSMD_PATH_SLAB)
-        bulk_kernel<Q, T, TG, 3><<<nblk, blk, bulk_dyn_smem<Q, T, 3>(), st>>>(a, gmap, fmap);
-    else
+    else if (path == SSMD_PATH_SLAB) {
+        if constexpr (kSlabs) bulk_kernel<Q, T, TG, 3><<<nblk, blk, bulk_dyn_smem<Q, T, 3>(), st>>>(a, gmap, fmap);
+    } else
         bulk_kernel<Q, T, TG, 1><<<nblk, blk, 0, st>>>(a, gmap, fmap);
     if (ev1) cudaEventRecord(ev1, st);
     if (int e = cuda_check(cudaGetLastError(), "bulk_kernel launch")) return e;

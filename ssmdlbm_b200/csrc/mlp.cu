@@ -1,30 +1,41 @@
 // mlp.cu — the learned closure's per-cell network on the 5th-generation tensor cores.
 //
-// Network: 12 features -> 64 -> 64 -> 2 outputs, GELU (erf form) after the
-// two hidden layers, features standardised by stored mean / inverse std,
-// outputs  p = scale * r + offset  with r the last layer's raw output.
-// A persistent CTA of 128 threads per SM loops over tiles of 128 cells
-// (thread i <-> cell row i of the tile), weights staged once per CTA:
+// Network: 12 features -> 64 -> 64 -> 2 outputs, GELU after the two hidden
+// layers in its tanh form, gelu(z) = z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715
+// z^3))) (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016), with
+// tanh from the SFU (tanh.approx.f32, absolute error about 2^-11, below the
+// bf16 rounding of the hidden activations that follows), features
+// standardised by stored mean / inverse std, outputs p = scale * r + offset
+// with r the last layer's raw output.  A persistent CTA of 128 threads loops
+// over tiles of 128 cells (thread i <-> cell row i of the tile), weights
+// staged once per CTA:
 //   X [128 x 16] (bf16, K padded 12 -> 16)   z1 = X W1^T      (tcgen05, N = 64, K = 16)
 //   H1 = gelu(z1 + b1) [128 x 64] bf16        z2 = H1 W2^T     (4 MMAs of K = 16)
 //   H2 = gelu(z2 + b2) [128 x 64] bf16        r  = H2 W3^T     (N padded 2 -> 16)
-// Accumulators live in TMEM (z1: columns 0-63, z2: 64-127, r: 128-143 when
-// training, 0-15 otherwise); the
-// epilogues read them back with tcgen05.ld, add the bias, apply GELU and
-// write the next layer's bf16 operand into shared memory.
-// Training (ssmd_mlp_grad) continues in the same CTA with the loss
-//   L = (1/n) sum_i sum_k w_ik (r_ik - (t_ik - offset_k) / scale_k)^2
-// and its backward pass: dH2 = dR W3 and dZ2 = dH2 gelu'(z2 + b2) on the CUDA
-// cores (N = 2 is too narrow for an MMA), dH1 = dZ2 W2 on the tensor cores
-// (TMEM columns 192-255), dZ1 = dH1 gelu'(z1 + b1); the weight and bias
-// gradients (sums over a tile's 128 rows) on the CUDA cores in FP32,
-// carried in registers across the CTA's tiles and added across CTAs with
-// atomics once at the end.  Every wait on an MMA is bounded:
-// on timeout the CTA records bit 0 of the status word, frees its TMEM and
-// returns.
+// The epilogues read the accumulators back with tcgen05.ld, add the bias,
+// apply GELU on pairs of columns with packed FP32 arithmetic (fma.rn.f32x2
+// and friends, sm_100) and write the next layer's bf16 operand.
+// Inference (forward, and the fused closure refresh that computes the
+// features from the macroscopic fields and applies the outputs) keeps one
+// 64-column accumulator (z1, z2 and r in turn: each is dead once its
+// epilogue has read it) and one activation tile (X, H1, H2 in turn: each is
+// dead once the MMA reading it has completed), 29 KB of shared memory and 64
+// TMEM columns per CTA, so seven CTAs share an SM and hide each other's MMA
+// round trips.
+// Training (ssmd_mlp_grad) keeps z1 and z2 for the backward pass:
+//   L = (1/n) sum_i sum_k w_ik (r_ik - (t_ik - offset_k) / scale_k)^2,
+// dH2 = dR W3 and dZ2 = dH2 gelu'(z2 + b2) on the CUDA cores (N = 2 is too
+// narrow for an MMA), dH1 = dZ2 W2 on the tensor cores, dZ1 = dH1 gelu'(z1 +
+// b1); the weight and bias gradients (sums over a tile's 128 rows) on the
+// CUDA cores in FP32, carried in registers across the CTA's tiles, then
+// either added across CTAs with atomics (ssmd_mlp_grad) or written as one row
+// per CTA and summed in CTA order by a second kernel (ssmd_mlp_grad_ws:
+// the same bits on every run).  Every wait on an MMA is bounded: on timeout
+// the CTA records bit 0 of the status word, frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "closure.cuh"
 #include "host.cuh"
 #include "umma.cuh"
 
@@ -42,37 +53,81 @@ constexpr int oMean = kParams, oInvStd = oMean + kIn, oScale = oInvStd + kIn, oO
 static_assert(kParams == SSMD_MLP_PARAMS, "parameter layout");
 static_assert(kNet == SSMD_MLP_NET_FLOATS, "network layout");
 
-// TMEM columns: training keeps z1 and z2 for the backward pass (256 columns);
-// inference writes the last layer over z1, which is dead by then (128
-// columns), so four inference CTAs fit on an SM's 512 columns.
-template <bool TRAIN>
-constexpr uint32_t tmem_cols() { return TRAIN ? 256u : 128u; }
-template <bool TRAIN>
-constexpr uint32_t col_r() { return TRAIN ? 128u : 0u; }
-constexpr uint32_t cZ1 = 0, cZ2 = 64, cDH1 = 192;
-constexpr int kFwdCtasPerSm = 4;
+enum : int { kFwd = 0, kTrain = 1, kRefresh = 2 };
+
+// TMEM columns: training keeps z1 (0-63) and z2 (64-127) for the backward
+// pass, r at 128-143 and dH1 at 192-255; inference puts z1, z2 and r in turn
+// on columns 0-63.
+template <int MODE>
+constexpr uint32_t tmem_cols() { return MODE == kTrain ? 256u : 64u; }
+template <int MODE>
+constexpr uint32_t col_z2() { return MODE == kTrain ? 64u : 0u; }
+template <int MODE>
+constexpr uint32_t col_r() { return MODE == kTrain ? 128u : 0u; }
+constexpr uint32_t cZ1 = 0, cDH1 = 192;
 constexpr uint64_t kMmaWaitNs = 1000000000ull;
 constexpr int kLd = 65; // fp32 row stride of the dZ staging arrays (bank-conflict free)
+constexpr int kMaxGradCtas = 256; // rows of the deterministic gradient workspace
 
-// shared-memory map (bytes from a 1024-aligned base)
-constexpr uint32_t sX = 0, sW1 = 4096, sW3 = 6144, sH1 = 8192, sW2 = 24576, sH2 = 32768, sFwdEnd = 49152;
+// shared-memory map (bytes from a 1024-aligned base); training-only tiles:
+// W2^T, bf16 dZ2, FP32 dZ2 and dZ1 staging, dL/dr
 constexpr uint32_t sW2T = 49152, sDZ2 = 57344, sDZ2F = 73728, sDZ1F = sDZ2F + kRows * kLd * 4,
-                   sDY = sDZ1F + kRows * kLd * 4, sTrainEnd = sDY + kRows * kOut * 4;
-
-template <bool TRAIN>
+                   sDY = sDZ1F + kRows * kLd * 4;
+template <int MODE>
 struct Layout {
-    static constexpr uint32_t small = TRAIN ? sTrainEnd : sFwdEnd;
-    static constexpr uint32_t b1 = small, b2 = b1 + kH * 4, b3 = b2 + kH * 4, w3f = b3 + 16,
-                              norm = w3f + kOut * kH * 4, bar = norm + 32 * 4, slot = bar + 8, abort = slot + 4,
-                              end = abort + 4;
+    static constexpr bool T = MODE == kTrain;
+    // inference: W1, W3, W2, then one activation tile that holds X, H1, H2 in turn
+    static constexpr uint32_t sW1 = T ? 4096 : 0, sW3 = T ? 6144 : 2048, sH1 = T ? 8192 : 12288,
+                              sW2 = T ? 24576 : 4096, sH2 = T ? 32768 : sH1, sX = T ? 0 : sH1;
+    static constexpr uint32_t big = T ? sDY + kRows * kOut * 4 : sH1 + kRows * kH * 2;
+    static constexpr uint32_t b1 = big, b2 = b1 + kH * 4, b3 = b2 + kH * 4, w3f = b3 + 16,
+                              norm = w3f + (T ? kOut * kH * 4 : 0), bar = norm + 32 * 4, slot = bar + 8,
+                              abort = slot + 4, end = abort + 4;
     static constexpr size_t bytes = end + 1024; // + alignment slack of the dynamic base
+};
+
+// Everything a launch needs (one struct for the three modes).
+struct MlpArgs {
+    const float *net;
+    const float *feat;   // kFwd, kTrain: n x 12 features
+    const float *target; // kTrain
+    const float *weight; // kTrain (may be null)
+    int64_t n;
+    float *out;          // kFwd: n x 2
+    float *grad;         // kTrain: atomics into grad, or null with partials
+    float *partials;     // kTrain deterministic: one row of kParams + 1 per CTA
+    double *loss;        // kTrain (atomic path)
+    closure::Grid g;     // kRefresh: the lattice and its macroscopic fields
+    const float *rho, *ux, *uy, *uz, *phi;
+    float nu_w, nu_dow, nut_max;
+    float *nut, *cs;     // kRefresh outputs
 };
 
 __device__ unsigned int g_mlp_status;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU, tanh form: u = sqrt(2/pi) z (1 + 0.044715 z^2), gelu = z/2 + z/2 tanh(u)
+constexpr float kG0 = 0.7978845608028654f;           // sqrt(2 / pi)
+constexpr float kG1 = 0.7978845608028654f * 0.044715f;
+
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// gelu of two columns at once: u = z fma(kG1, z^2, kG0), h = z/2,
+// gelu = fma(h, tanh(u), h), elementwise with packed FP32 (fma.rn.f32x2 etc.)
+__device__ __forceinline__ float2 gelu2(float2 z) {
+    const float2 p = __ffma2_rn(__fmul2_rn(z, z), make_float2(kG1, kG1), make_float2(kG0, kG0));
+    const float2 u = __fmul2_rn(z, p);
+    const float2 hz = __fmul2_rn(z, make_float2(0.5f, 0.5f));
+    return __ffma2_rn(hz, make_float2(tanh_sfu(u.x), tanh_sfu(u.y)), hz);
+}
+// d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) du/dz,  du/dz = sqrt(2/pi) (1 + 3 * 0.044715 z^2)
 __device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    const float z2 = z * z;
+    const float t = tanh_sfu(z * fmaf(kG1, z2, kG0));
+    const float du = fmaf(3.0f * kG1, z2, kG0);
+    return fmaf(0.5f * z * du, fmaf(-t, t, 1.0f), fmaf(0.5f, t, 0.5f));
 }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -121,23 +176,62 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bia
     for (int c = 0; c < 4; ++c) {
         float v[16];
         umma::tmem_ld16(taddr + 16 * c, v);
+        uint32_t pk[8];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + bias[16 * c + i]);
-        st8(tile, r, 16 * c, kH, v);
-        st8(tile, r, 16 * c + 8, kH, v + 8);
+        for (int i = 0; i < 4; ++i) {
+            const float4 b = *reinterpret_cast<const float4 *>(bias + 16 * c + 4 * i);
+            const float2 g0 = gelu2(__fadd2_rn(make_float2(v[4 * i], v[4 * i + 1]), make_float2(b.x, b.y)));
+            const float2 g1 = gelu2(__fadd2_rn(make_float2(v[4 * i + 2], v[4 * i + 3]), make_float2(b.z, b.w)));
+            pk[2 * i] = pack2(g0.x, g0.y);
+            pk[2 * i + 1] = pack2(g1.x, g1.y);
+        }
+        *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(r, 16 * c, kH)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(r, 16 * c + 8, kH)) =
+            make_uint4(pk[4], pk[5], pk[6], pk[7]);
     }
 }
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
-    mlp_kernel(const float *__restrict__ net, const float *__restrict__ feat, const float *__restrict__ target,
-               const float *__restrict__ weight, int64_t n, float *__restrict__ out, float *__restrict__ grad,
-               double *__restrict__ loss) {
-    using L = Layout<TRAIN>;
+// The 12 standardised features of one row into x[16] (columns 12-15 zero);
+// kRefresh also returns feature 11, nu(phi), for the bound on nu_t.
+template <int MODE>
+__device__ __forceinline__ void load_row(const MlpArgs &a, const float *norm, int64_t row, bool valid, float (&x)[kK1],
+                                         float &nu_phi) {
+#pragma unroll
+    for (int i = 0; i < kK1; ++i) x[i] = 0.f;
+    nu_phi = 0.f;
+    if (!valid) return;
+    float f[kIn];
+    if constexpr (MODE == kRefresh) {
+        closure::cell_features(a.g, a.rho, a.ux, a.uy, a.uz, a.phi, a.nu_w, a.nu_dow, row, f);
+    } else if ((reinterpret_cast<uintptr_t>(a.feat) & 15u) == 0) {
+        const float4 *p = reinterpret_cast<const float4 *>(a.feat + row * kIn); // 48-byte rows: 16-byte aligned
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const float4 v = __ldg(p + q);
+            f[4 * q] = v.x;
+            f[4 * q + 1] = v.y;
+            f[4 * q + 2] = v.z;
+            f[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) f[i] = __ldg(a.feat + row * kIn + i);
+    }
+    nu_phi = f[11];
+#pragma unroll
+    for (int i = 0; i < kIn; ++i) x[i] = (f[i] - norm[i]) * norm[kIn + i];
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 6) mlp_kernel(const MlpArgs a) {
+    constexpr bool TRAIN = MODE == kTrain;
+    using L = Layout<MODE>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                           ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5;
+    const float *net = a.net;
+    const int64_t n = a.n;
     float *b1 = reinterpret_cast<float *>(sm + L::b1);
     float *b2 = reinterpret_cast<float *>(sm + L::b2);
     float *b3 = reinterpret_cast<float *>(sm + L::b3);
@@ -147,22 +241,23 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
     uint32_t *slot = reinterpret_cast<uint32_t *>(sm + L::slot);
     volatile uint32_t *abort_flag = reinterpret_cast<volatile uint32_t *>(sm + L::abort);
 
-    // ---- set-up: TMEM, barrier, weights, this CTA's features
-    if (warp == 0) umma::tmem_alloc(slot, tmem_cols<TRAIN>());
+    // ---- set-up: TMEM, barrier, weights
+    if (warp == 0) umma::tmem_alloc(slot, tmem_cols<MODE>());
     if (tid == 0) {
         mbar_init(bar, 1);
         *abort_flag = 0u;
         fence_barrier_init();
     }
-    load_weights(sm + sW1, net + oW1, kH, kH, kK1, false, tid);
-    load_weights(sm + sW2, net + oW2, kH, kH, kH, false, tid);
-    load_weights(sm + sW3, net + oW3, kOut, kN3, kH, false, tid);
+    load_weights(sm + L::sW1, net + oW1, kH, kH, kK1, false, tid);
+    load_weights(sm + L::sW2, net + oW2, kH, kH, kH, false, tid);
+    load_weights(sm + L::sW3, net + oW3, kOut, kN3, kH, false, tid);
     if constexpr (TRAIN) load_weights(sm + sW2T, net + oW2, kH, kH, kH, true, tid); // (i, o) = W2[o][i]
     for (int e = tid; e < kH; e += kThreadsMlp) {
         b1[e] = net[oB1 + e];
         b2[e] = net[oB2 + e];
     }
-    for (int e = tid; e < kOut * kH; e += kThreadsMlp) w3f[e] = net[oW3 + e];
+    if constexpr (TRAIN)
+        for (int e = tid; e < kOut * kH; e += kThreadsMlp) w3f[e] = net[oW3 + e];
     if (tid < kOut) b3[tid] = net[oB3 + tid];
     if (tid < kNet - kParams) norm[tid] = net[kParams + tid];
     __syncthreads();
@@ -186,16 +281,12 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
     for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const int64_t row = tile * kRows + r;
         const bool valid = row < n;
+        float nu_phi;
         {
             float x[kK1];
-#pragma unroll
-            for (int i = 0; i < kK1; ++i) {
-                float v = 0.f;
-                if (i < kIn && valid) v = (feat[row * kIn + i] - norm[i]) * norm[kIn + i];
-                x[i] = v;
-            }
-            st8(sm + sX, r, 0, kK1, x);
-            st8(sm + sX, r, 8, kK1, x + 8);
+            load_row<MODE>(a, norm, row, valid, x, nu_phi);
+            st8(sm + L::sX, r, 0, kK1, x);
+            st8(sm + L::sX, r, 8, kK1, x + 8);
         }
         fence_proxy_async(); // generic-proxy smem writes -> visible to the tensor core
         umma::fence_before_sync();
@@ -206,14 +297,14 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
         // ---- layer 1
         if (tid == 0) {
             umma::fence_after_sync();
-            umma::mma_bf16(tmem + cZ1, umma::smem_desc(sbase + sX, 128, 256),
-                           umma::smem_desc(sbase + sW1, 128, 256), umma::idesc_bf16(128, kH), false);
+            umma::mma_bf16(tmem + cZ1, umma::smem_desc(sbase + L::sX, 128, 256),
+                           umma::smem_desc(sbase + L::sW1, 128, 256), umma::idesc_bf16(128, kH), false);
             umma::commit(bar);
         }
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue(lane_base + cZ1, b1, sm + sH1, r);
+        hidden_epilogue(lane_base + cZ1, b1, sm + L::sH1, r);
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
@@ -222,15 +313,15 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
         if (tid == 0) {
             umma::fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
-                umma::mma_bf16(tmem + cZ2, umma::smem_desc(sbase + sH1 + 256 * ks, 128, 1024),
-                               umma::smem_desc(sbase + sW2 + 256 * ks, 128, 1024), umma::idesc_bf16(128, kH),
+                umma::mma_bf16(tmem + col_z2<MODE>(), umma::smem_desc(sbase + L::sH1 + 256 * ks, 128, 1024),
+                               umma::smem_desc(sbase + L::sW2 + 256 * ks, 128, 1024), umma::idesc_bf16(128, kH),
                                ks > 0);
             umma::commit(bar);
         }
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue(lane_base + cZ2, b2, sm + sH2, r);
+        hidden_epilogue(lane_base + col_z2<MODE>(), b2, sm + L::sH2, r);
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
@@ -239,8 +330,8 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
         if (tid == 0) {
             umma::fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
-                umma::mma_bf16(tmem + col_r<TRAIN>(), umma::smem_desc(sbase + sH2 + 256 * ks, 128, 1024),
-                               umma::smem_desc(sbase + sW3 + 256 * ks, 128, 1024), umma::idesc_bf16(128, kN3),
+                umma::mma_bf16(tmem + col_r<MODE>(), umma::smem_desc(sbase + L::sH2 + 256 * ks, 128, 1024),
+                               umma::smem_desc(sbase + L::sW3 + 256 * ks, 128, 1024), umma::idesc_bf16(128, kN3),
                                ks > 0);
             umma::commit(bar);
         }
@@ -249,15 +340,24 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
         if (!ok) break;
         float rr[kOut];
         {
-            float v[16];
-            umma::tmem_ld16(lane_base + col_r<TRAIN>(), v);
+            float v[2];
+            umma::tmem_ld2(lane_base + col_r<MODE>(), v);
             rr[0] = v[0] + b3[0];
             rr[1] = v[1] + b3[1];
         }
-        if constexpr (!TRAIN) {
+        if constexpr (MODE == kFwd) {
+            if (valid)
+                *reinterpret_cast<float2 *>(a.out + row * kOut) =
+                    make_float2(fmaf(norm[2 * kIn + 0], rr[0], norm[2 * kIn + 2]),
+                                fmaf(norm[2 * kIn + 1], rr[1], norm[2 * kIn + 3]));
+        } else if constexpr (MODE == kRefresh) {
+            // the closure's bounds (ssmd_closure_apply): nu_t >= max(-nu(phi)/2, -nut_max)
             if (valid) {
-                out[row * kOut + 0] = fmaf(norm[2 * kIn + 0], rr[0], norm[2 * kIn + 2]);
-                out[row * kOut + 1] = fmaf(norm[2 * kIn + 1], rr[1], norm[2 * kIn + 3]);
+                const float p0 = fmaf(norm[2 * kIn + 0], rr[0], norm[2 * kIn + 2]);
+                const float p1 = fmaf(norm[2 * kIn + 1], rr[1], norm[2 * kIn + 3]);
+                const float lo = fmaxf(-0.5f * nu_phi, -a.nut_max);
+                a.nut[row] = fminf(fmaxf(p0, lo), a.nut_max);
+                a.cs[row] = fminf(fmaxf(p1, 0.25f), 4.0f);
             }
         } else {
             float *dzf2 = reinterpret_cast<float *>(sm + sDZ2F);
@@ -267,10 +367,10 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
             float d0 = 0.f, d1 = 0.f;
             if (valid) {
                 const float inv_n = 1.0f / (float)n;
-                const float t0 = (target[row * kOut + 0] - norm[2 * kIn + 2]) / norm[2 * kIn + 0];
-                const float t1 = (target[row * kOut + 1] - norm[2 * kIn + 3]) / norm[2 * kIn + 1];
-                const float w0 = weight ? weight[row * kOut + 0] : 1.0f;
-                const float w1 = weight ? weight[row * kOut + 1] : 1.0f;
+                const float t0 = (a.target[row * kOut + 0] - norm[2 * kIn + 2]) / norm[2 * kIn + 0];
+                const float t1 = (a.target[row * kOut + 1] - norm[2 * kIn + 3]) / norm[2 * kIn + 1];
+                const float w0 = a.weight ? a.weight[row * kOut + 0] : 1.0f;
+                const float w1 = a.weight ? a.weight[row * kOut + 1] : 1.0f;
                 const float e0 = rr[0] - t0, e1 = rr[1] - t1;
                 lsum += w0 * e0 * e0 + w1 * e1 * e1;
                 d0 = 2.0f * w0 * e0 * inv_n;
@@ -282,7 +382,7 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 float v[16];
-                umma::tmem_ld16(lane_base + cZ2 + 16 * c, v);
+                umma::tmem_ld16(lane_base + col_z2<MODE>() + 16 * c, v);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     const int j = 16 * c + i;
@@ -324,7 +424,7 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
                     const float d = dzf2[rr2 * kLd + o];
 #pragma unroll
                     for (int ch = 0; ch < 4; ++ch) {
-                        const uint4 u = *reinterpret_cast<const uint4 *>(sm + sH1 +
+                        const uint4 u = *reinterpret_cast<const uint4 *>(sm + L::sH1 +
                                                                          umma::kmajor_offset(rr2, i0 + 8 * ch, kH));
                         const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
 #pragma unroll
@@ -340,7 +440,7 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
                 const int o = tid >> 1, i0 = (tid & 1) * 8;
                 for (int rr2 = 0; rr2 < kRows; ++rr2) {
                     const float d = dzf1[rr2 * kLd + o];
-                    const uint4 u = *reinterpret_cast<const uint4 *>(sm + sX + umma::kmajor_offset(rr2, i0, kK1));
+                    const uint4 u = *reinterpret_cast<const uint4 *>(sm + L::sX + umma::kmajor_offset(rr2, i0, kK1));
                     const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
@@ -353,7 +453,7 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
             {   // dW3[k][j] = sum_r dR[r][k] H2[r][j]; db2 (k = 0 threads), db1 (k = 1); db3
                 const int k = tid >> 6, j = tid & 63;
                 for (int rr2 = 0; rr2 < kRows; ++rr2) {
-                    gw3 = fmaf(dy[rr2 * kOut + k], ldbf(sm + sH2, rr2, j, kH), gw3);
+                    gw3 = fmaf(dy[rr2 * kOut + k], ldbf(sm + L::sH2, rr2, j, kH), gw3);
                     gb += k == 0 ? dzf2[rr2 * kLd + j] : dzf1[rr2 * kLd + j];
                 }
                 if (tid < kOut)
@@ -365,20 +465,33 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
 
     if constexpr (TRAIN) {
         if (ok) {
+            // atomics into grad, or this CTA's row of the deterministic workspace
+            float *dst = a.partials ? a.partials + (size_t)blockIdx.x * (kParams + 1) : a.grad;
+            auto put = [&](int k, float v) {
+                if (a.partials) dst[k] = v;
+                else atomicAdd(&dst[k], v);
+            };
             const int o = tid >> 1;
             const int i0 = (tid & 1) * 32, i1 = (tid & 1) * 8;
 #pragma unroll
-            for (int i = 0; i < 32; ++i) atomicAdd(&grad[oW2 + o * kH + i0 + i], gw2[i]);
+            for (int i = 0; i < 32; ++i) put(oW2 + o * kH + i0 + i, gw2[i]);
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                if (i1 + i < kIn) atomicAdd(&grad[oW1 + o * kK1 + i1 + i], gw1[i]);
+            for (int i = 0; i < 8; ++i) put(oW1 + o * kK1 + i1 + i, i1 + i < kIn ? gw1[i] : 0.f);
             const int k = tid >> 6, j = tid & 63;
-            atomicAdd(&grad[oW3 + k * kH + j], gw3);
-            atomicAdd(&grad[(k == 0 ? oB2 : oB1) + j], gb);
-            if (tid < kOut) atomicAdd(&grad[oB3 + tid], gb3);
+            put(oW3 + k * kH + j, gw3);
+            put((k == 0 ? oB2 : oB1) + j, gb);
+            if (tid < kOut) put(oB3 + tid, gb3);
             float l = lsum;
             for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
-            if ((tid & 31) == 0) atomicAdd(loss, (double)l / (double)n);
+            if (a.partials) {
+                float *wl = reinterpret_cast<float *>(sm + sDY); // per-warp losses, summed in warp order
+                __syncthreads();
+                if ((tid & 31) == 0) wl[warp] = l;
+                __syncthreads();
+                if (tid == 0) dst[kParams] = ((wl[0] + wl[1]) + wl[2]) + wl[3];
+            } else if ((tid & 31) == 0) {
+                atomicAdd(a.loss, (double)l / (double)n);
+            }
         }
     }
 
@@ -386,7 +499,24 @@ __global__ void __launch_bounds__(kThreadsMlp, TRAIN ? 1 : kFwdCtasPerSm)
     umma::fence_before_sync();
     __syncthreads();
     if (!ok && tid == 0) atomicOr(&g_mlp_status, 1u);
-    if (warp == 0) umma::tmem_dealloc(*slot, tmem_cols<TRAIN>());
+    if (warp == 0) umma::tmem_dealloc(*slot, tmem_cols<MODE>());
+}
+
+// Deterministic reduction of the per-CTA gradient rows: thread k sums column
+// k over the CTAs in CTA order (FP32, like the atomic path); the loss column
+// in FP64.
+__global__ void grad_sum_kernel(const float *__restrict__ partials, int ctas, int64_t n, float *__restrict__ grad,
+                                double *__restrict__ loss) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < kParams) {
+        float s = 0.f;
+        for (int b = 0; b < ctas; ++b) s += partials[(size_t)b * (kParams + 1) + k];
+        grad[k] = s;
+    } else if (k == kParams) {
+        double s = 0.0;
+        for (int b = 0; b < ctas; ++b) s += (double)partials[(size_t)b * (kParams + 1) + kParams];
+        *loss = s / (double)n;
+    }
 }
 
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
@@ -402,34 +532,53 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
     p[i] -= lr * (mi / corr1) / (sqrtf(vi / corr2) + eps);
 }
 
-template <bool TRAIN>
-int launch(const float *net, const float *feat, const float *target, const float *weight, int64_t n, float *out,
-           float *grad, double *loss, cudaStream_t st) {
-    // shared memory sized so that at most 512 / tmem_cols CTAs share an SM:
-    // every resident CTA then holds its TMEM columns without waiting in
-    // tcgen05.alloc (training: 1 per SM, inference: 4 per SM)
-    const size_t floor_bytes = TRAIN ? (size_t)120 * 1024 : (size_t)52 * 1024;
-    const size_t smem = Layout<TRAIN>::bytes > floor_bytes ? Layout<TRAIN>::bytes : floor_bytes;
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (int e = cuda_check(cudaFuncSetAttribute(mlp_kernel<TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// Resident CTAs per SM of a mode (occupancy query once per mode and device)
+// and the SM count.
+template <int MODE>
+int launch_shape(size_t smem, int &per_sm, int &sms) {
+    static thread_local int cached_dev = -1, c_per_sm = 1, c_sms = 148;
+    int dev = 0;
+    if (int e = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return e;
+    if (dev != cached_dev) {
+        if (int e = cuda_check(cudaFuncSetAttribute(mlp_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                     (int)smem),
                                "mlp smem attribute"))
             return e;
-        attr_set = true;
+        int nb = 0, m = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mlp_kernel<MODE>, kThreadsMlp, smem) != cudaSuccess ||
+            nb <= 0)
+            nb = 1;
+        if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || m <= 0) m = 148;
+        // TMEM: every resident CTA must get its columns without waiting in tcgen05.alloc
+        const int tmem_limit = (int)(512u / tmem_cols<MODE>());
+        c_per_sm = nb < tmem_limit ? nb : tmem_limit;
+        c_sms = m;
+        cached_dev = dev;
     }
-    // persistent: one CTA per SM, each loops over 128-row tiles
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-    }
-    const int64_t tiles = (n + kRows - 1) / kRows;
-    const int64_t slots = (int64_t)sms * (TRAIN ? 1 : kFwdCtasPerSm);
+    per_sm = c_per_sm;
+    sms = c_sms;
+    return SSMD_OK;
+}
+
+template <int MODE>
+int launch(MlpArgs a, cudaStream_t st, int max_ctas = 0) {
+    // training: one CTA per SM (its 256 TMEM columns and ~120 KB of shared memory)
+    const size_t smem = MODE == kTrain ? (Layout<MODE>::bytes > (size_t)120 * 1024 ? Layout<MODE>::bytes
+                                                                                     : (size_t)120 * 1024)
+                                       : Layout<MODE>::bytes;
+    int per_sm = 1, sms = 148;
+    if (int e = launch_shape<MODE>(smem, per_sm, sms)) return e;
+    const int64_t tiles = (a.n + kRows - 1) / kRows;
+    int64_t slots = (int64_t)sms * per_sm;
+    if (max_ctas > 0 && slots > max_ctas) slots = max_ctas;
     const unsigned blocks = (unsigned)(tiles < slots ? tiles : slots);
-    mlp_kernel<TRAIN><<<blocks, kThreadsMlp, smem, st>>>(net, feat, target, weight, n, out, grad, loss);
-    return cuda_check(cudaGetLastError(), "mlp launch");
+    mlp_kernel<MODE><<<blocks, kThreadsMlp, smem, st>>>(a);
+    if (int e = cuda_check(cudaGetLastError(), "mlp launch")) return e;
+    if (MODE == kTrain && a.partials) {
+        grad_sum_kernel<<<(kParams + 1 + 255) / 256, 256, 0, st>>>(a.partials, (int)blocks, a.n, a.grad, a.loss);
+        return cuda_check(cudaGetLastError(), "gradient sum launch");
+    }
+    return SSMD_OK;
 }
 
 } // namespace
@@ -439,8 +588,13 @@ extern "C" int ssmd_mlp_forward(const float *net, const float *features, int64_t
     if (!net || !features || !out || n < 0) return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument or n < 0");
     if (n == 0) return SSMD_OK;
     if (n > (int64_t)0x7FFFFFFF * kRows) return fail(SSMD_ERR_INVALID_ARGUMENT, "too many rows");
-    return launch<false>(net, features, nullptr, nullptr, n, out, nullptr, nullptr,
-                         reinterpret_cast<cudaStream_t>(stream));
+    if ((reinterpret_cast<uintptr_t>(out) & 7u) != 0) return fail(SSMD_ERR_INVALID_ARGUMENT, "out must be 8-byte aligned");
+    MlpArgs a{};
+    a.net = net;
+    a.feat = features;
+    a.n = n;
+    a.out = out;
+    return launch<kFwd>(a, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ssmd_mlp_grad(const float *net, const float *features, const float *targets, const float *weights,
@@ -451,7 +605,63 @@ extern "C" int ssmd_mlp_grad(const float *net, const float *features, const floa
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (int e = cuda_check(cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st), "grad clear")) return e;
     if (int e = cuda_check(cudaMemsetAsync(loss, 0, sizeof(double), st), "loss clear")) return e;
-    return launch<true>(net, features, targets, weights, n, nullptr, grad, loss, st);
+    MlpArgs a{};
+    a.net = net;
+    a.feat = features;
+    a.target = targets;
+    a.weight = weights;
+    a.n = n;
+    a.grad = grad;
+    a.loss = loss;
+    return launch<kTrain>(a, st);
+}
+
+extern "C" size_t ssmd_mlp_grad_workspace_bytes(void) {
+    return sizeof(float) * (size_t)kMaxGradCtas * (kParams + 1);
+}
+
+extern "C" int ssmd_mlp_grad_ws(const float *net, const float *features, const float *targets, const float *weights,
+                                int64_t n, float *grad, double *loss, float *workspace, size_t workspace_bytes,
+                                ssmd_stream_t stream) {
+    if (!net || !features || !targets || !grad || !loss || !workspace || n <= 0)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument or n <= 0");
+    if (n > (int64_t)0x7FFFFFFF * kRows) return fail(SSMD_ERR_INVALID_ARGUMENT, "too many rows");
+    if (workspace_bytes < ssmd_mlp_grad_workspace_bytes())
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "workspace_bytes %zu < required %zu", workspace_bytes,
+                    ssmd_mlp_grad_workspace_bytes());
+    MlpArgs a{};
+    a.net = net;
+    a.feat = features;
+    a.target = targets;
+    a.weight = weights;
+    a.n = n;
+    a.grad = grad;
+    a.loss = loss;
+    a.partials = workspace;
+    return launch<kTrain>(a, reinterpret_cast<cudaStream_t>(stream), kMaxGradCtas);
+}
+
+extern "C" int ssmd_closure_refresh(const ssmd_params *coarse, const LBMFields *fields, const float *net,
+                                    float nut_max, float *nut, float *sigma_scale, ssmd_stream_t stream) {
+    if (int e = ssmd_validate(coarse)) return e;
+    if (!fields || !fields->rho || !fields->ux || !fields->uy || !fields->uz || !fields->phi || !net || !nut ||
+        !sigma_scale)
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument");
+    MlpArgs a{};
+    a.net = net;
+    a.n = (int64_t)coarse->nx * coarse->ny * coarse->nz;
+    a.g = closure::grid_of(*coarse);
+    a.rho = fields->rho;
+    a.ux = fields->ux;
+    a.uy = fields->uy;
+    a.uz = fields->uz;
+    a.phi = fields->phi;
+    a.nu_w = coarse->nu_water;
+    a.nu_dow = coarse->nu_oil - coarse->nu_water;
+    a.nut_max = nut_max;
+    a.nut = nut;
+    a.cs = sigma_scale;
+    return launch<kRefresh>(a, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ssmd_mlp_adam(float *net, const float *grad, float *m, float *v, int64_t t, float lr, float beta1,

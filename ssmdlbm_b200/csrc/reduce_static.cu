@@ -153,6 +153,7 @@ extern "C" int ssmd_reduce_static(const ssmd_params *p, const LBMFields *fields,
     switch (p->storage) {
     case SSMD_STORAGE_F32: e = reduce_static<float>(*p, *fields, steps_done, v, st); break;
     case SSMD_STORAGE_F16: e = reduce_static<__half>(*p, *fields, steps_done, v, st); break;
+    case SSMD_STORAGE_F16_G32: e = reduce_static<half_g32>(*p, *fields, steps_done, v, st); break;
     default: e = reduce_static<__nv_bfloat16>(*p, *fields, steps_done, v, st); break;
     }
     if (e) return e;

@@ -60,9 +60,11 @@ void profile_free() {
 SSMD_DECLARE(19, float)
 SSMD_DECLARE(19, __half)
 SSMD_DECLARE(19, __nv_bfloat16)
+SSMD_DECLARE(19, half_g32)
 SSMD_DECLARE(27, float)
 SSMD_DECLARE(27, __half)
 SSMD_DECLARE(27, __nv_bfloat16)
+SSMD_DECLARE(27, half_g32)
 
 } // namespace host
 } // namespace ssmd
@@ -114,10 +116,10 @@ size_t ssmd_scalar_bytes(const ssmd_params *p) {
     return p ? (size_t)p->nx * p->ny * p->nz * sizeof(float) : 0;
 }
 size_t ssmd_f_bytes(const ssmd_params *p) {
-    return p ? (size_t)p->nx * p->ny * p->nz * (size_t)p->velocity_set * storage_size(p->storage) : 0;
+    return p ? (size_t)p->nx * p->ny * p->nz * (size_t)p->velocity_set * f_storage_size(p->storage) : 0;
 }
 size_t ssmd_g_bytes(const ssmd_params *p) {
-    return p ? (size_t)p->nx * p->ny * p->nz * 7u * storage_size(p->storage) : 0;
+    return p ? (size_t)p->nx * p->ny * p->nz * 7u * g_storage_size(p->storage) : 0;
 }
 size_t ssmd_workspace_bytes(const ssmd_params *p) {
     (void)p;
@@ -129,7 +131,7 @@ int ssmd_validate(const ssmd_params *p) {
     if (p->velocity_set != 19 && p->velocity_set != 27)
         return fail(SSMD_ERR_INVALID_ARGUMENT, "velocity_set must be 19 or 27 (got %d)",
                     p->velocity_set);
-    if (p->storage < SSMD_STORAGE_F32 || p->storage > SSMD_STORAGE_BF16)
+    if (p->storage < SSMD_STORAGE_F32 || p->storage > SSMD_STORAGE_F16_G32)
         return fail(SSMD_ERR_INVALID_ARGUMENT, "unknown storage %d", p->storage);
     if (p->bc_x != SSMD_BC_PERIODIC_COPY && p->bc_x != SSMD_BC_PERIODIC)
         return fail(SSMD_ERR_INVALID_ARGUMENT, "bc_x must be PERIODIC_COPY or PERIODIC");
@@ -242,6 +244,8 @@ int ssmd_init_from_macros(const ssmd_params *p, LBMFields *fields, ssmd_stream_t
     case 27 * 4 + SSMD_STORAGE_F32: e = launch_init_pops<27, float>(*p, *fields, st); break;
     case 27 * 4 + SSMD_STORAGE_F16: e = launch_init_pops<27, __half>(*p, *fields, st); break;
     case 27 * 4 + SSMD_STORAGE_BF16: e = launch_init_pops<27, __nv_bfloat16>(*p, *fields, st); break;
+    case 19 * 4 + SSMD_STORAGE_F16_G32: e = launch_init_pops<19, half_g32>(*p, *fields, st); break;
+    case 27 * 4 + SSMD_STORAGE_F16_G32: e = launch_init_pops<27, half_g32>(*p, *fields, st); break;
     default: return fail(SSMD_ERR_UNSUPPORTED, "unsupported velocity set / storage");
     }
     if (e) return e;
@@ -267,6 +271,8 @@ int ssmd_step(LBMFields *fields, const ssmd_params *p, uint64_t step, uint32_t f
     case 27 * 4 + SSMD_STORAGE_F16: return launch_step<27, __half>(*p, *fields, step, flags, st);
     case 27 * 4 + SSMD_STORAGE_BF16:
         return launch_step<27, __nv_bfloat16>(*p, *fields, step, flags, st);
+    case 19 * 4 + SSMD_STORAGE_F16_G32: return launch_step<19, half_g32>(*p, *fields, step, flags, st);
+    case 27 * 4 + SSMD_STORAGE_F16_G32: return launch_step<27, half_g32>(*p, *fields, step, flags, st);
     default: return fail(SSMD_ERR_UNSUPPORTED, "unsupported velocity set / storage");
     }
 }
@@ -323,6 +329,7 @@ int ssmd_reduce(const ssmd_params *p, const LBMFields *fields, uint64_t steps_do
     switch (p->storage) {
     case SSMD_STORAGE_F32: e = launch_reduce<float>(*p, *fields, steps_done, v, st); break;
     case SSMD_STORAGE_F16: e = launch_reduce<__half>(*p, *fields, steps_done, v, st); break;
+    case SSMD_STORAGE_F16_G32: e = launch_reduce<half_g32>(*p, *fields, steps_done, v, st); break;
     default: e = launch_reduce<__nv_bfloat16>(*p, *fields, steps_done, v, st); break;
     }
     if (e) return e;
@@ -352,7 +359,7 @@ int ssmd_populations_to_push(const ssmd_params *p, const LBMFields *fields, uint
     const bool even = (steps_done & 1ull) == 0ull;
     const void *src = which == 0 ? (even ? fields->f : p->f_alt) : (even ? fields->g : p->g_alt);
     if (which == 1) {
-        if (p->storage == SSMD_STORAGE_F32) return launch_to_push<float, 7>(*p, src, out, st);
+        if (g_storage_size(p->storage) == 4) return launch_to_push<float, 7>(*p, src, out, st);
         return launch_to_push<unsigned short, 7>(*p, src, out, st);
     }
     const bool f32 = p->storage == SSMD_STORAGE_F32;

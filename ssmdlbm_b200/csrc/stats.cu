@@ -276,6 +276,9 @@ extern "C" int ssmd_phase_flux(const ssmd_params *p, const LBMFields *fields, ui
     switch (p->storage) {
     case SSMD_STORAGE_F32: phase_flux_kernel<float><<<nb, 256, 0, st>>>(G, static_cast<const float *>(g), acc); break;
     case SSMD_STORAGE_F16: phase_flux_kernel<__half><<<nb, 256, 0, st>>>(G, static_cast<const __half *>(g), acc); break;
+    case SSMD_STORAGE_F16_G32: // g as float
+        phase_flux_kernel<float><<<nb, 256, 0, st>>>(G, static_cast<const float *>(g), acc);
+        break;
     default: { // BF16 runs keep g in half
         using TG = phase_t<__nv_bfloat16>;
         phase_flux_kernel<TG><<<nb, 256, 0, st>>>(G, static_cast<const TG *>(g), acc);

@@ -91,6 +91,10 @@ struct TmaType<__half> {
     static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
 };
 template <>
+struct TmaType<half_g32> {
+    static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+};
+template <>
 struct TmaType<__nv_bfloat16> {
     static constexpr CUtensorMapDataType value = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
 };

@@ -19,11 +19,12 @@ from . import _lib
 from ._lib import LBMFields, Params, Stats, check, lib
 
 STORAGE_DTYPES = {_lib.STORAGE_F32: torch.float32, _lib.STORAGE_F16: torch.float16,
-                  _lib.STORAGE_BF16: torch.bfloat16}
+                  _lib.STORAGE_BF16: torch.bfloat16, _lib.STORAGE_F16_G32: torch.float16}
 # element type of the phase populations g: BF16 runs keep g in half (phi in
-# [0, 1] needs mantissa bits, not range)
+# [0, 1] needs mantissa bits, not range); F16_G32 keeps it in float, as the
+# reference's FP16 build does
 PHASE_DTYPES = {_lib.STORAGE_F32: torch.float32, _lib.STORAGE_F16: torch.float16,
-                _lib.STORAGE_BF16: torch.float16}
+                _lib.STORAGE_BF16: torch.float16, _lib.STORAGE_F16_G32: torch.float32}
 SCALARS = ("rho", "ux", "uy", "uz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz", "phi", "fsx", "fsy", "fsz")
 
 

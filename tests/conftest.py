@@ -22,4 +22,5 @@ def _built():
     from oracle import build as obuild
     pbuild.build()
     obuild.build_oracle()
+    obuild.build_oracle_gpu()
     yield

@@ -85,6 +85,41 @@ def test_gradient_matches_oracle():
     assert _status() == 0
 
 
+def test_reproducible_gradient_matches_the_atomic_one():
+    """ssmd_mlp_grad_ws (one row per CTA, summed in CTA order) gives the same
+    bits on every call, and the atomic ssmd_mlp_grad's values to FP32
+    summation order; on 300 000 rows (many tiles per CTA)."""
+    rng = np.random.default_rng(7)
+    n = 300_000
+    net = _net(4)
+    feat = rng.normal(0, 1.5, (n, co.IN)).astype(np.float32)
+    tgt = np.stack([rng.uniform(0, 0.02, n), rng.uniform(0.5, 2, n)], 1).astype(np.float32)
+    dn, df, dt = _dev(net), _dev(feat), _dev(tgt)
+    L = lib()
+    ws = torch.empty(L.ssmd_mlp_grad_workspace_bytes() // 4, device="cuda")
+    out = []
+    for _ in range(2):
+        grad = torch.empty(co.PARAMS, device="cuda")
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        check(L.ssmd_mlp_grad_ws(dn.data_ptr(), df.data_ptr(), dt.data_ptr(), None, n, grad.data_ptr(),
+                                 loss.data_ptr(), ws.data_ptr(), ws.numel() * 4, None))
+        torch.cuda.synchronize()
+        out.append((grad.cpu().numpy(), loss.item()))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+    ga = torch.empty(co.PARAMS, device="cuda")
+    la = torch.zeros(1, dtype=torch.float64, device="cuda")
+    check(L.ssmd_mlp_grad(dn.data_ptr(), df.data_ptr(), dt.data_ptr(), None, n, ga.data_ptr(), la.data_ptr(), None))
+    torch.cuda.synchronize()
+    g0, ga = out[0][0].astype(np.float64), ga.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(g0 - ga) <= 1e-5 * np.linalg.norm(ga)
+    assert abs(out[0][1] - la.item()) <= 1e-6 * la.item()
+    small = torch.empty(16, device="cuda")
+    rc = L.ssmd_mlp_grad_ws(dn.data_ptr(), df.data_ptr(), dt.data_ptr(), None, n, small.data_ptr(),
+                            la.data_ptr(), small.data_ptr(), 64, None)
+    assert rc == _lib.SSMD_ERR_INVALID_ARGUMENT  # workspace too small
+    assert _status() == 0
+
+
 def test_adam_matches_oracle():
     rng = np.random.default_rng(2)
     net = _net(3)
@@ -223,3 +258,39 @@ def test_closure_arrays_enter_the_step():
     assert np.all(np.isfinite(visc["uz"]))
     surf, st2 = _closure_run(0.0, 2.0)
     assert st2 == 0 and not np.array_equal(plain["ux"], surf["ux"])
+
+
+def test_fused_refresh_equals_features_then_apply():
+    """ssmd_closure_refresh (features, network and bounds in one kernel)
+    gives the nu_t and sigma factor of ssmd_closure_features followed by
+    ssmd_closure_apply, on a jet lattice of 40 960 cells (a partial last
+    tile), with a network whose outputs reach both bounds."""
+    from ssmdlbm_b200.lbm import Simulation
+    p = configs.oil_jet(32, 32, 40, 19, tau=0.55, sigma=1e-3, mobility=0.1, diam=8, w_in=0.05, noise=0.01, seed=4)
+    s = Simulation(p)
+    s.init()
+    s.step(60, store_macros=True)
+    n = s.cells + 0
+    net = _net(6)
+    net[co.oScale:co.oOffset] = [0.05, 3.0]  # wide outputs: the clamps are exercised
+    dn = _dev(net)
+    feat = torch.empty(n, co.IN, device="cuda")
+    out = torch.empty(n, 2, device="cuda")
+    nut_a, cs_a = torch.empty(n, device="cuda"), torch.empty(n, device="cuda")
+    nut_b, cs_b = torch.empty(n, device="cuda"), torch.empty(n, device="cuda")
+    L = lib()
+    pr, fl = ctypes.byref(s.p), ctypes.byref(s.fields)
+    check(L.ssmd_closure_features(pr, fl, feat.data_ptr(), s.stream))
+    check(L.ssmd_closure_apply(pr, dn.data_ptr(), feat.data_ptr(), out.data_ptr(), nut_a.data_ptr(),
+                               cs_a.data_ptr(), 0.02, s.stream))
+    check(L.ssmd_closure_refresh(pr, fl, dn.data_ptr(), 0.02, nut_b.data_ptr(), cs_b.data_ptr(), s.stream))
+    torch.cuda.synchronize()
+    a, b = nut_a.cpu().numpy(), nut_b.cpu().numpy()
+    c, d = cs_a.cpu().numpy(), cs_b.cpu().numpy()
+    # the features are the same function on both paths; where the compiler
+    # contracts one of them differently a bf16 operand may round the other way
+    assert np.mean(a == b) >= 0.99 and np.mean(c == d) >= 0.99
+    assert np.abs(a - b).max() <= 1e-2 * np.abs(a).max() and np.abs(c - d).max() <= 1e-2 * np.abs(c).max()
+    assert (c == 4.0).any() or (c == 0.25).any() or (a == 0.02).any()  # a bound was reached
+    assert _status() == 0
+    s.close()

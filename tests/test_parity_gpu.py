@@ -223,7 +223,8 @@ def test_nonfinite_state_is_reported():
         sim.reduce()
 
 
-@pytest.mark.parametrize("storage,tol", [(_lib.STORAGE_F16, 5e-3), (_lib.STORAGE_BF16, 5e-2)])
+@pytest.mark.parametrize("storage,tol", [(_lib.STORAGE_F16, 5e-3), (_lib.STORAGE_BF16, 5e-2),
+                                         (_lib.STORAGE_F16_G32, 5e-3)])
 def test_reduced_storage_error_vs_fp64_oracle(storage, tol):
     p = harness_params("q19_s", periodic_y=True, storage=storage)
     macros = seeded_macros((p.nz, p.ny, p.nx), seed=21)
