@@ -234,8 +234,16 @@ STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2, "f16g32": 3}
 
 # DRAM bytes per cell of one bulk launch on the 128 x 128 x 512 jet,
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of that
-# launch (profiles/), keyed by (velocity set, storage)
-NCU_BYTES_PER_CELL = {(27, "f32"): 278.5, (19, "f32"): 214.4, (27, "f16"): 133.7}
+# launch, keyed by (velocity set, storage): (bytes, the profiles/ summary
+# that records the capture, the commit of the captured build).  The bulk
+# kernel's device code of these instantiations has not changed since the
+# commits named; a change to bulk.cuh or lattice.cuh calls for a new capture
+# and new entries here.
+NCU_BYTES_PER_CELL = {
+    (27, "f32"): (278.5, "profiles/bulk_kernel_q27_f32_oil_jet.md", "9cd0754"),
+    (19, "f32"): (214.4, "profiles/bulk_kernel_q19_f32_oil_jet.md", "9cd0754"),
+    (27, "f16"): (133.7, "profiles/bulk_kernel_q27_f16_oil_jet.md", "fa907c4"),
+}
 
 
 def time_graph(sim, steps: int, warmup: int, world: int):
@@ -354,27 +362,25 @@ def cpu_baseline(p, steps: int = 3):
                       f"warm-up step ({dt:.1f} s)"}
 
 
-def run_sweep(steps: int = 40):
+def run_sweep(steps: int = 2000):
     """The 48-lattice sweep (N x N x 4N, N in {32, 48, 64, 96}, seed 2; D3Q19
-    f32): batched persistent launches replayed as graphs, z-chunk height
-    tuned over {8, 16, 32, 48, 64}, against the same steps issued lattice by
-    lattice."""
+    f32) for its 2000 steps: batched persistent launches replayed as graphs,
+    the z-chunk height from the autotuner (autotune.tune_sweep), against the
+    same steps issued lattice by lattice."""
     import torch
+    from ssmdlbm_b200 import autotune
     from ssmdlbm_b200.batch import Sweep, sweep_params
     sw = Sweep(sweep_params(48, seed=2))
+    tuned = autotune.tune_sweep(sw)
     sw.init()
-    best = None
-    for tz in (8, 16, 32, 48, 64):
-        sw.set_tile_z(tz)
-        sw.timed(4)
-        dt = sw.timed(steps)
-        if best is None or dt < best[1]:
-            best = (tz, dt)
-    sw.set_tile_z(best[0])
+    sw.timed(4)
+    dt = sw.timed(steps)
     sw.timed_one_by_one(4)
     dt_single = sw.timed_one_by_one(steps)
-    out = {"lattices": sw.count, "cells": sw.cells, "steps": steps, "tile_z": best[0],
-           "batched_mlups": round(sw.cells * steps / best[1] / 1e6, 1),
+    out = {"lattices": sw.count, "cells": sw.cells, "steps": steps, "tile_z": int(sw.tile_z),
+           "tile_z_from": "autotune.tune_sweep", "tuning": tuned.get("tried"),
+           "all_lattices_ok": all(s.check_status() == 0 for s in sw.sims),
+           "batched_mlups": round(sw.cells * steps / dt / 1e6, 1),
            "one_by_one_mlups": round(sw.cells * steps / dt_single / 1e6, 1),
            "launches_per_step": {"batched": 3, "one_by_one": sw.count * 2}}
     sw.close()
@@ -405,14 +411,16 @@ def mlp_throughput(net=None, rows: int = 1 << 24, reps: int = 20):
     st = torch.cuda.current_stream().cuda_stream
     n_ptr, g_ptr, l_ptr = net.net.data_ptr(), net.grad.data_ptr(), net.loss.data_ptr()
 
-    def timed(fn, n_reps):
+    def timed(fn, n_reps, stream=None):
+        """Mean device seconds of fn(), CUDA events on the stream it launches on."""
+        stream = stream or torch.cuda.current_stream()
         for _ in range(3):
             fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(stream)
         for _ in range(n_reps):
             fn()
-        e1.record()
+        e1.record(stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / 1e3 / n_reps
 
@@ -439,8 +447,8 @@ def mlp_throughput(net=None, rows: int = 1 << 24, reps: int = 20):
     nut, cs = torch.empty(n, device="cuda"), torch.empty(n, device="cuda")
     pr, fl = ct.byref(sim.p), ct.byref(sim.fields)
     s_per = timed(lambda: _lib.check(L.ssmd_closure_refresh(pr, fl, n_ptr, 0.05, nut.data_ptr(), cs.data_ptr(),
-                                                             sim.stream)), 10)
-    step_s = timed(lambda: sim.step(1), 10)
+                                                             sim.stream)), 10, sim.torch_stream)
+    step_s = timed(lambda: sim.step(1), 10, sim.torch_stream)
     res["refresh_fused"] = {"cells": n, "g_cells_per_s": round(n / s_per / 1e9, 3), "ms": round(s_per * 1e3, 4),
                             "tflops": round(flop_row * n / s_per / 1e12, 2),
                             "coarse_step_ms": round(step_s * 1e3, 4),
@@ -720,8 +728,11 @@ def run_ours(a, world, rank, local):
                    "l2": "inputs larger than L2 (populations 0.9 GB per buffer)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "traffic": (int(NCU_BYTES_PER_CELL[(a.vs, a.storage)] * NX * NY * NZ)
+                     "traffic": (int(NCU_BYTES_PER_CELL[(a.vs, a.storage)][0] * NX * NY * NZ)
                                  if (a.vs, a.storage) in NCU_BYTES_PER_CELL and not a.size else None),
+                     "traffic_source": ("ncu capture of one launch on this lattice: {}, build {}".format(
+                         *NCU_BYTES_PER_CELL[(a.vs, a.storage)][1:])
+                         if (a.vs, a.storage) in NCU_BYTES_PER_CELL and not a.size else None),
                      "peak_kind": peak_kind, "kernel": f"ssmd::bulk_kernel<{a.vs},{a.storage}>",
                      "bytes_per_cell": b_alg(a.vs, s_f0, s_g0), "launch_ms": round(bulk_ms, 4)},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),

@@ -110,3 +110,44 @@ def tune(sim, steps: int = 10, force: bool = False, verbose: bool = False) -> di
     sim.p.bulk_path, sim.p.tile_z = path, tz
     sim.init()
     return best
+
+
+# z chunks tried for a batched sweep (the work items of all lattices share one
+# persistent launch, so the chunk trades items per lattice against prologues)
+SWEEP_TILE_Z = (8, 12, 16, 24, 32, 48, 64)
+
+
+def sweep_signature(sw) -> str:
+    import hashlib
+    sigs = ",".join(signature(p) for p in sw.params)
+    return f"sweep{sw.count}-" + hashlib.sha1(sigs.encode()).hexdigest()[:16]
+
+
+def tune_sweep(sw, steps: int = 10, force: bool = False, verbose: bool = False) -> dict:
+    """Measure the batched step of a sweep (a batch.Sweep) over SWEEP_TILE_Z,
+    set the fastest on it and cache it (same file and device key as tune()).
+    The populations are scratch for the search: re-initialise the sweep
+    afterwards."""
+    import torch
+    dev = torch.cuda.get_device_name(sw.device)
+    key = f"{dev}|{sweep_signature(sw)}"
+    cache = _load()
+    if not force and key in cache:
+        best = cache[key]
+        sw.set_tile_z(int(best["tile_z"]))
+        return best
+    results = []
+    for tz in SWEEP_TILE_Z:
+        sw.set_tile_z(tz)
+        sw.timed(2)  # warm-up and graph capture
+        dt = sw.timed(steps)
+        results.append((dt / steps * 1e3, tz))
+        if verbose:
+            print(f"autotune sweep tile_z={tz}: {dt / steps * 1e3:.4f} ms/step")
+    ms, tz = min(results)
+    sw.set_tile_z(tz)
+    best = {"tile_z": tz, "ms_per_step": ms, "tried": [{"tile_z": t, "ms": round(m, 5)} for m, t in sorted(results)]}
+    cache = _load()
+    cache[key] = best
+    _save(cache)
+    return best
