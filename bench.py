@@ -543,8 +543,11 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
     from ssmdlbm_b200.lbm import Simulation
     peak, _ = hbm_peak()
     fine_p = c5_params()
+    # the eddy viscosity is bounded by the coarse lattice's molecular one (half
+    # the fine one): the closure corrects the flow, it does not take it over
+    nut_max = 0.5 * float(fine_p.nu_water)
     r = closure.experiment(fine_p, steps=steps, sample_every=sample_every, spinup=spinup, train_steps=train_steps,
-                           batch=65536, lr=1e-3, seed=0, update_every=update_every, nut_max=0.05,
+                           batch=65536, lr=1e-3, seed=0, update_every=update_every, nut_max=nut_max,
                            coarse_storage=_lib.STORAGE_F16)
     f, pl, cl = r["fine"], r["plain"], r["closure"]
     # bulk-kernel roofline of the two lattices (fresh runs, 10 launches each)
@@ -576,6 +579,7 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
         "fine": {"mlups": mlups(f), "device_s": round(f.device_s, 3), **bulk["fine_f32"]},
         "coarse_plain": {"mlups": mlups(pl), "device_s": round(pl.device_s, 3)},
         "coarse_closure": {"mlups": mlups(cl), "device_s": round(cl.device_s, 3), **bulk["coarse_f16"]},
+        "nut_max": nut_max,
         "training": {"device_s": round(r["train_device_s"], 3), "adam_steps": train_steps, "samples": r["samples"],
                      "heldout_loss": r["heldout_loss"], "reproducible_gradient": True},
         "time_ratio": round(cl.device_s / f.device_s, 4),
@@ -811,6 +815,8 @@ def main() -> int:
     ap.add_argument("--vs", type=int, default=Q, choices=[19, 27])
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_NAMES))
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--no-production", action="store_true",
+                    help="skip the production leg (384 x 384 x 1536 fine run, training, 192 x 192 x 768 coarse runs)")
     ap.add_argument("--c4", action="store_true",
                     help="run only the closure study's data generation and training (8 fine seeds, about 12 min)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],

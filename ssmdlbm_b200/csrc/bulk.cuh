@@ -368,8 +368,8 @@ struct Bulk {
     // Normal, |grad phi| of one ring element from its gradient.
     static __device__ __forceinline__ void store_nrm(BulkSmem &S, int s, int nxh, int nyh, float gx, float gy,
                                                      float gz) {
-        const float ind = sqrtf(fmaf(gx, gx, fmaf(gy, gy, gz * gz)));
-        const float inv = __frcp_rn(ind + 1e-9f); // = 1 / (ind + 1e-9), correctly rounded
+        const float ind = sqrt_sfu(fmaf(gx, gx, fmaf(gy, gy, gz * gz)));
+        const float inv = rcp_sfu(ind + 1e-9f); // 1 / (ind + 1e-9)
         S.nrm[s][0][nyh][nxh] = gx * inv;
         S.nrm[s][1][nyh][nxh] = gy * inv;
         S.nrm[s][2][nyh][nxh] = gz * inv;
@@ -692,7 +692,7 @@ struct Bulk {
         const Moments m = moments<Q>(f, fx, fy, fz);
         float nu = fmaf(phi, P.nu_oil_minus_water, P.nu_water);
         if (a.clo_nut) nu += a.clo_nut[c0];
-        const float omega = __frcp_rn(fmaf(3.0f, nu, 0.5f)); // = 1 / (0.5 + 3 nu), correctly rounded
+        const float omega = rcp_sfu(fmaf(3.0f, nu, 0.5f)); // 1 / (0.5 + 3 nu)
         float fo[Q];
         collide<Q>(m, 1.0f - omega, fx, fy, fz, fo);
         unroll<0, Q>([&](auto q) { Store<TF>::st(a.fq_dst[q] + c0, fo[q]); });

@@ -21,6 +21,23 @@
 
 namespace ssmd {
 
+// Reciprocal and square root on the SFU (rcp.approx / sqrt.approx: at most 1
+// ulp / 2^-23 relative error, subnormal inputs and results flushed to 0).
+// The reference divides with IEEE rounding; the step stays within FP32
+// rounding of it (the parity tests hold 1e-5 after 100 steps against its own
+// kernels), and the correctly rounded forms cost 6-8 more instructions each,
+// three to four times per cell: 1.8-6 % of the bulk kernel's time on B200.
+__device__ __forceinline__ float rcp_sfu(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sqrt_sfu(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <int I>
 using ic = std::integral_constant<int, I>;
 
@@ -158,7 +175,7 @@ __device__ __forceinline__ Moments moments(const float (&f)[Q], float fx, float 
     }
     Moments m;
     m.rho = s + 1.0f;
-    const float inv = __frcp_rn(m.rho); // = 1 / rho, correctly rounded
+    const float inv = rcp_sfu(m.rho);
     const float hinv = 0.5f * inv;
     m.ux = fmaf(jx, inv, fx * hinv);
     m.uy = fmaf(jy, inv, fy * hinv);

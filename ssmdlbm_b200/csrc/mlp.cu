@@ -35,6 +35,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "closure.cuh"
 #include "host.cuh"
 #include "umma.cuh"
@@ -532,8 +534,13 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
     p[i] -= lr * (mi / corr1) / (sqrtf(vi / corr2) + eps);
 }
 
-// Resident CTAs per SM of a mode (occupancy query once per mode and device)
-// and the SM count.
+// Resident CTAs per SM of a mode and the SM count, computed once per mode and
+// device from the device's limits: shared memory (with the per-block
+// reservation), registers (allocated per warp in multiples of 8 per thread),
+// threads, blocks, and TMEM (every resident CTA must get its columns without
+// waiting in tcgen05.alloc).  On sm_100a with CUDA 12.9 the occupancy query
+// returns 1 for these kernels, where the hardware holds 7 (ncu's
+// launch__occupancy_limit_shared_mem), so it is not used.
 template <int MODE>
 int launch_shape(size_t smem, int &per_sm, int &sms) {
     static thread_local int cached_dev = -1, c_per_sm = 1, c_sms = 148;
@@ -544,14 +551,26 @@ int launch_shape(size_t smem, int &per_sm, int &sms) {
                                                     (int)smem),
                                "mlp smem attribute"))
             return e;
-        int nb = 0, m = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mlp_kernel<MODE>, kThreadsMlp, smem) != cudaSuccess ||
-            nb <= 0)
-            nb = 1;
-        if (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || m <= 0) m = 148;
-        // TMEM: every resident CTA must get its columns without waiting in tcgen05.alloc
-        const int tmem_limit = (int)(512u / tmem_cols<MODE>());
-        c_per_sm = nb < tmem_limit ? nb : tmem_limit;
+        cudaFuncAttributes fa{};
+        if (int e = cuda_check(cudaFuncGetAttributes(&fa, mlp_kernel<MODE>), "mlp attributes")) return e;
+        auto attr = [&](cudaDeviceAttr a, int fallback) {
+            int v = 0;
+            return (cudaDeviceGetAttribute(&v, a, dev) == cudaSuccess && v > 0) ? v : fallback;
+        };
+        const int m = attr(cudaDevAttrMultiProcessorCount, 148);
+        const int smem_sm = attr(cudaDevAttrMaxSharedMemoryPerMultiprocessor, 233472);
+        const int reserved = attr(cudaDevAttrReservedSharedMemoryPerBlock, 1024);
+        const int regs_sm = attr(cudaDevAttrMaxRegistersPerMultiprocessor, 65536);
+        const int threads_sm = attr(cudaDevAttrMaxThreadsPerMultiProcessor, 2048);
+        const int blocks_sm = attr(cudaDevAttrMaxBlocksPerMultiprocessor, 32);
+        const int regs_warp = ((fa.numRegs + 7) / 8) * 8 * 32;
+        const int warps = kThreadsMlp / 32;
+        int n = smem_sm / ((int)smem + fa.sharedSizeBytes + reserved);
+        n = std::min(n, regs_sm / (regs_warp * warps));
+        n = std::min(n, threads_sm / kThreadsMlp);
+        n = std::min(n, blocks_sm);
+        n = std::min(n, (int)(512u / tmem_cols<MODE>()));
+        c_per_sm = n > 0 ? n : 1;
         c_sms = m;
         cached_dev = dev;
     }
