@@ -550,10 +550,23 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
                            batch=65536, lr=1e-3, seed=0, update_every=update_every, nut_max=nut_max,
                            coarse_storage=_lib.STORAGE_F16)
     f, pl, cl = r["fine"], r["plain"], r["closure"]
-    # bulk-kernel roofline of the two lattices (fresh runs, 10 launches each)
-    bulk = {}
     cp = closure.coarse_params(fine_p)
     cp.storage = _lib.STORAGE_F16
+    # ablation: the trained network with one of its two outputs held at the
+    # plain method's value (output scale 0, offset nu_t = 0 or factor 1)
+    ablation = {}
+    P, I = _lib.MLP_PARAMS, _lib.MLP_IN
+    for name, k, value in (("nut_only", 1, 1.0), ("sigma_only", 0, 0.0)):
+        part = closure.Network(0)
+        part.net.copy_(r["net"].net)
+        part.net[P + 2 * I + k] = 0.0
+        part.net[P + 2 * I + 2 + k] = value
+        s = closure.coarse_run(cp, steps // 2, max(1, sample_every // 2), spinup // 2, part, update_every, nut_max)
+        ablation[name] = {key: closure.stat_errors(s, f)[key] for key in ("centreline_uz", "centreline_phi",
+                                                                          "phi_volume")}
+        del part
+    # bulk-kernel roofline of the two lattices (fresh runs, 10 launches each)
+    bulk = {}
     for name, p, s_f in (("fine_f32", fine_p, 4), ("coarse_f16", cp, 2)):
         sim = Simulation(p)
         sim.init()
@@ -586,6 +599,7 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
         "time_ratio_plain_coarse": round(pl.device_s / f.device_s, 4),
         "errors_vs_filtered_fine": {k: {"plain": r["errors_plain"][k], "closure": r["errors_closure"][k]}
                                     for k in keys},
+        "closure_ablation": ablation,
         "fine_droplets_per_snapshot": f.droplets_mean,
         "mlp_status": r["mlp_status"],
         "mlp": mlp_throughput(net),

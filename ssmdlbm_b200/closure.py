@@ -412,3 +412,60 @@ def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train
         "train_curve": curve, "train_device_s": train_s, "samples": int(feats.shape[0]),
         "wall_s": time.perf_counter() - t0, "mlp_status": net.status(), "net": net,
     }
+
+
+def throughput(rows: int = 1 << 22, coarse=(96, 96, 192), reps: int = 3) -> dict:
+    """Device throughput of the closure network: `reps` forward launches on
+    `rows` random feature rows, then `reps` fused refreshes of a coarse D3Q27
+    jet lattice of shape `coarse` (FP16 storage), CUDA events on the streams
+    the launches use."""
+    from .lbm import Simulation
+    from . import configs
+    L = lib()
+    net = Network(0)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    feats = torch.randn(rows, _lib.MLP_IN, device="cuda", generator=g)
+    out = torch.empty(rows, 2, device="cuda")
+    cur = torch.cuda.current_stream()
+
+    def timed(fn, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    t_fwd = timed(lambda: check(L.ssmd_mlp_forward(net.net.data_ptr(), feats.data_ptr(), rows, out.data_ptr(),
+                                                   cur.cuda_stream)), cur)
+    del feats, out
+    nx, ny, nz = coarse
+    cp = configs.oil_jet(nx, ny, nz, 27, tau=0.51, sigma=5e-4, width=2.0, mobility=0.05, diam=12, w_in=0.06,
+                         noise=0.01, seed=3, storage=_lib.STORAGE_F16)
+    sim = Simulation(cp)
+    sim.init()
+    sim.step(2, store_macros=True)
+    nut = torch.empty(sim.cells, device=sim.device)
+    cs = torch.empty(sim.cells, device=sim.device)
+    t_ref = timed(lambda: check(L.ssmd_closure_refresh(ctypes.byref(sim.p), ctypes.byref(sim.fields),
+                                                       net.net.data_ptr(), 0.05, nut.data_ptr(), cs.data_ptr(),
+                                                       sim.stream)), sim.torch_stream)
+    cells = sim.cells
+    sim.close()
+    flop_row = 2 * (12 * 64 + 64 * 64 + 64 * 2)
+    return {"forward": {"rows": rows, "g_rows_per_s": rows / t_fwd / 1e9, "tflops": flop_row * rows / t_fwd / 1e12},
+            "refresh": {"cells": cells, "g_cells_per_s": cells / t_ref / 1e9, "ms": t_ref * 1e3},
+            "status": net.status()}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="throughput of the closure network's kernels")
+    ap.add_argument("--rows", type=int, default=1 << 22, help="feature rows of the forward launches")
+    ap.add_argument("--coarse", default="96,96,192", help="nx,ny,nz of the refreshed coarse lattice")
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    print(json.dumps(throughput(a.rows, tuple(int(v) for v in a.coarse.split(",")), a.reps)))
