@@ -430,6 +430,7 @@ def throughput(rows: int = 1 << 22, coarse=(96, 96, 192), reps: int = 3) -> dict
     cur = torch.cuda.current_stream()
 
     def timed(fn, stream):
+        fn()  # warm-up: module load and launch set-up stay out of the timing
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):

@@ -48,21 +48,47 @@ __device__ __forceinline__ void strain(const Grid &g, const float *ux, const flo
     grad3(g, uz, x, y, z, d[2][0], d[2][1], d[2][2]);
 }
 
+// The six face neighbours of a cell, as 32-bit cell indices (a lattice has
+// fewer than 2^32 cells): the same cells nbr() and idx() give, found with one
+// 32-bit division chain per cell instead of 64-bit arithmetic per load.
+struct Faces {
+    uint32_t xp, xm, yp, ym, zp, zm;
+};
+
+__device__ __forceinline__ Faces faces(const Grid &g, uint32_t c) {
+    const uint32_t nx = (uint32_t)g.nx, nxy = nx * (uint32_t)g.ny;
+    const uint32_t z = c / nxy, rxy = c - z * nxy, y = rxy / nx, x = rxy - y * nx;
+    // step d along an axis of n cells at coordinate v, stride s: wrap or clamp like nbr()
+    auto up = [](uint32_t v, uint32_t n, uint32_t s, bool per) { return v + 1 < n ? s : (per ? s - n * s : 0u); };
+    auto dn = [](uint32_t v, uint32_t n, uint32_t s, bool per) { return v > 0 ? 0u - s : (per ? n * s - s : 0u); };
+    Faces f;
+    f.xp = c + up(x, nx, 1u, g.px);
+    f.xm = c + dn(x, nx, 1u, g.px);
+    f.yp = c + up(y, (uint32_t)g.ny, nx, g.py);
+    f.ym = c + dn(y, (uint32_t)g.ny, nx, g.py);
+    f.zp = c + up(z, (uint32_t)g.nz, nxy, g.pz);
+    f.zm = c + dn(z, (uint32_t)g.nz, nxy, g.pz);
+    return f;
+}
+
 // The SSMD_MLP_IN features of cell i.
 __device__ __forceinline__ void cell_features(const Grid &g, const float *rho, const float *ux, const float *uy,
                                               const float *uz, const float *phi, float nu_w, float nu_dow, int64_t i,
                                               float (&f)[SSMD_MLP_IN]) {
-    const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((int64_t)g.nx * g.ny));
+    const Faces n6 = faces(g, (uint32_t)i);
     const float ph = phi[i];
-    float gx, gy, gz;
-    grad3(g, phi, x, y, z, gx, gy, gz);
+    auto diff = [&](const float *a, uint32_t p, uint32_t m) { return 0.5f * (a[p] - a[m]); };
+    const float gx = diff(phi, n6.xp, n6.xm), gy = diff(phi, n6.yp, n6.ym), gz = diff(phi, n6.zp, n6.zm);
     const float gmag = sqrtf(gx * gx + gy * gy + gz * gz);
-    const float lap = phi[idx(g, nbr(x, 1, g.nx, g.px), y, z)] + phi[idx(g, nbr(x, -1, g.nx, g.px), y, z)] +
-                      phi[idx(g, x, nbr(y, 1, g.ny, g.py), z)] + phi[idx(g, x, nbr(y, -1, g.ny, g.py), z)] +
-                      phi[idx(g, x, y, nbr(z, 1, g.nz, g.pz))] + phi[idx(g, x, y, nbr(z, -1, g.nz, g.pz))] -
-                      6.0f * ph;
+    const float lap = phi[n6.xp] + phi[n6.xm] + phi[n6.yp] + phi[n6.ym] + phi[n6.zp] + phi[n6.zm] - 6.0f * ph;
     float d[3][3];
-    strain(g, ux, uy, uz, x, y, z, d);
+    const float *u3[3] = {ux, uy, uz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        d[a][0] = diff(u3[a], n6.xp, n6.xm);
+        d[a][1] = diff(u3[a], n6.yp, n6.ym);
+        d[a][2] = diff(u3[a], n6.zp, n6.zm);
+    }
     float ss = 0.f, nsn = 0.f;
     const float inv = 1.0f / (gmag + 1e-9f);
     const float n[3] = {gx * inv, gy * inv, gz * inv};

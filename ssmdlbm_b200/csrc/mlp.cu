@@ -12,9 +12,13 @@
 //   X [128 x 16] (bf16, K padded 12 -> 16)   z1 = X W1^T      (tcgen05, N = 64, K = 16)
 //   H1 = gelu(z1 + b1) [128 x 64] bf16        z2 = H1 W2^T     (4 MMAs of K = 16)
 //   H2 = gelu(z2 + b2) [128 x 64] bf16        r  = H2 W3^T     (N padded 2 -> 16)
-// The epilogues read the accumulators back with tcgen05.ld, add the bias,
+// The epilogues read the accumulators back with tcgen05.ld (the next 16
+// columns in flight while the current 16 are processed), add the bias,
 // apply GELU on pairs of columns with packed FP32 arithmetic (fma.rn.f32x2
-// and friends, sm_100) and write the next layer's bf16 operand.
+// and friends, sm_100) and write the next layer's bf16 operand.  Inference
+// stages W2 and W3 halved and its epilogues write 2 gelu(z), one multiply
+// fewer per value: the products, hence every result, are the same bit for
+// bit (scaling by 2 commutes with each rounding).
 // Inference (forward, and the fused closure refresh that computes the
 // features from the macroscopic fields and applies the outputs) keeps one
 // 64-column accumulator (z1, z2 and r in turn: each is dead once its
@@ -71,7 +75,8 @@ constexpr uint64_t kMmaWaitNs = 1000000000ull;
 constexpr int kLd = 65; // fp32 row stride of the dZ staging arrays (bank-conflict free)
 constexpr int kMaxGradCtas = 256; // rows of the deterministic gradient workspace
 
-// shared-memory map (bytes from a 1024-aligned base); training-only tiles:
+// shared-memory map (bytes from an aligned base: 1024 bytes for training,
+// 128 for inference; the no-swizzle operand layout needs 16); training-only tiles:
 // W2^T, bf16 dZ2, FP32 dZ2 and dZ1 staging, dL/dr
 constexpr uint32_t sW2T = 49152, sDZ2 = 57344, sDZ2F = 73728, sDZ1F = sDZ2F + kRows * kLd * 4,
                    sDY = sDZ1F + kRows * kLd * 4;
@@ -85,7 +90,8 @@ struct Layout {
     static constexpr uint32_t b1 = big, b2 = b1 + kH * 4, b3 = b2 + kH * 4, w3f = b3 + 16,
                               norm = w3f + (T ? kOut * kH * 4 : 0), bar = norm + 32 * 4, slot = bar + 8,
                               abort = slot + 4, end = abort + 4;
-    static constexpr size_t bytes = end + 1024; // + alignment slack of the dynamic base
+    static constexpr uint32_t align = T ? 1024 : 128;
+    static constexpr size_t bytes = end + align; // + alignment slack of the dynamic base
 };
 
 // Everything a launch needs (one struct for the three modes).
@@ -117,12 +123,16 @@ __device__ __forceinline__ float tanh_sfu(float x) {
     return y;
 }
 // gelu of two columns at once: u = z fma(kG1, z^2, kG0), h = z/2,
-// gelu = fma(h, tanh(u), h), elementwise with packed FP32 (fma.rn.f32x2 etc.)
+// gelu = fma(h, tanh(u), h), elementwise with packed FP32 (fma.rn.f32x2 etc.);
+// TWICE: 2 gelu(z) = fma(z, tanh(u), z).
+template <bool TWICE = false>
 __device__ __forceinline__ float2 gelu2(float2 z) {
     const float2 p = __ffma2_rn(__fmul2_rn(z, z), make_float2(kG1, kG1), make_float2(kG0, kG0));
     const float2 u = __fmul2_rn(z, p);
+    const float2 t = make_float2(tanh_sfu(u.x), tanh_sfu(u.y));
+    if constexpr (TWICE) return __ffma2_rn(z, t, z);
     const float2 hz = __fmul2_rn(z, make_float2(0.5f, 0.5f));
-    return __ffma2_rn(hz, make_float2(tanh_sfu(u.x), tanh_sfu(u.y)), hz);
+    return __ffma2_rn(hz, t, hz);
 }
 // d gelu / dz = (1 + t)/2 + z/2 (1 - t^2) du/dz,  du/dz = sqrt(2/pi) (1 + 3 * 0.044715 z^2)
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -151,15 +161,16 @@ __device__ __forceinline__ float ldbf(const unsigned char *tile, int r, int k, i
     return __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(tile + umma::kmajor_offset(r, k, K)));
 }
 
-// Copy a [rows x K] block of fp32 weights (row stride K) into a bf16 tile
-// of rows_pad rows (extra rows zero); transpose: element (r, k) = src[k * rows + r].
+// Copy a [rows x K] block of fp32 weights (row stride K), times `scale` (a
+// power of two), into a bf16 tile of rows_pad rows (extra rows zero);
+// transpose: element (r, k) = src[k * rows + r].
 __device__ void load_weights(unsigned char *tile, const float *src, int rows, int rows_pad, int K, bool transpose,
-                             int tid) {
+                             int tid, float scale = 1.0f) {
     for (int e = tid; e < rows_pad * K; e += kThreadsMlp) {
         const int r = e / K, k = e % K;
         float v = 0.f;
         if (r < rows) v = transpose ? src[k * rows + r] : src[r * K + k];
-        *reinterpret_cast<__nv_bfloat16 *>(tile + umma::kmajor_offset(r, k, K)) = __float2bfloat16_rn(v);
+        *reinterpret_cast<__nv_bfloat16 *>(tile + umma::kmajor_offset(r, k, K)) = __float2bfloat16_rn(v * scale);
     }
 }
 
@@ -172,18 +183,27 @@ __device__ __forceinline__ bool wait_mma(uint64_t *bar, uint32_t phase, volatile
     return ok;
 }
 
-// Bias + GELU epilogue of a 64-column accumulator into a [128 x 64] bf16 tile.
+// Bias + GELU epilogue of a 64-column accumulator into a [128 x 64] bf16 tile
+// (TWICE: 2 gelu, for a next layer staged with halved weights).  The TMEM
+// load of columns 16 (c + 1) .. 16 c + 31 is in flight while columns 16 c ..
+// 16 c + 15 are processed.
+template <bool TWICE = false>
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bias, unsigned char *tile, int r) {
+    uint32_t nxt[16];
+    umma::tmem_ld16_issue(taddr, nxt);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         float v[16];
-        umma::tmem_ld16(taddr + 16 * c, v);
+        umma::tmem_ld_wait16(nxt);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(nxt[i]);
+        if (c < 3) umma::tmem_ld16_issue(taddr + 16 * (c + 1), nxt);
         uint32_t pk[8];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const float4 b = *reinterpret_cast<const float4 *>(bias + 16 * c + 4 * i);
-            const float2 g0 = gelu2(__fadd2_rn(make_float2(v[4 * i], v[4 * i + 1]), make_float2(b.x, b.y)));
-            const float2 g1 = gelu2(__fadd2_rn(make_float2(v[4 * i + 2], v[4 * i + 3]), make_float2(b.z, b.w)));
+            const float2 g0 = gelu2<TWICE>(__fadd2_rn(make_float2(v[4 * i], v[4 * i + 1]), make_float2(b.x, b.y)));
+            const float2 g1 = gelu2<TWICE>(__fadd2_rn(make_float2(v[4 * i + 2], v[4 * i + 3]), make_float2(b.z, b.w)));
             pk[2 * i] = pack2(g0.x, g0.y);
             pk[2 * i + 1] = pack2(g1.x, g1.y);
         }
@@ -225,12 +245,12 @@ __device__ __forceinline__ void load_row(const MlpArgs &a, const float *norm, in
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 6) mlp_kernel(const MlpArgs a) {
+__global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kernel(const MlpArgs a) {
     constexpr bool TRAIN = MODE == kTrain;
     using L = Layout<MODE>;
     extern __shared__ unsigned char smem_raw[];
-    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
-                                                          ~(uintptr_t)1023);
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + (L::align - 1)) &
+                                                          ~(uintptr_t)(L::align - 1));
     const int tid = threadIdx.x, warp = tid >> 5;
     const float *net = a.net;
     const int64_t n = a.n;
@@ -251,8 +271,9 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 6) mlp_kerne
         fence_barrier_init();
     }
     load_weights(sm + L::sW1, net + oW1, kH, kH, kK1, false, tid);
-    load_weights(sm + L::sW2, net + oW2, kH, kH, kH, false, tid);
-    load_weights(sm + L::sW3, net + oW3, kOut, kN3, kH, false, tid);
+    // inference feeds W2 and W3 with 2 gelu(z): halved weights, the same products
+    load_weights(sm + L::sW2, net + oW2, kH, kH, kH, false, tid, TRAIN ? 1.0f : 0.5f);
+    load_weights(sm + L::sW3, net + oW3, kOut, kN3, kH, false, tid, TRAIN ? 1.0f : 0.5f);
     if constexpr (TRAIN) load_weights(sm + sW2T, net + oW2, kH, kH, kH, true, tid); // (i, o) = W2[o][i]
     for (int e = tid; e < kH; e += kThreadsMlp) {
         b1[e] = net[oB1 + e];
@@ -306,7 +327,7 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 6) mlp_kerne
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue(lane_base + cZ1, b1, sm + L::sH1, r);
+        hidden_epilogue<!TRAIN>(lane_base + cZ1, b1, sm + L::sH1, r);
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
@@ -323,7 +344,7 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 6) mlp_kerne
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue(lane_base + col_z2<MODE>(), b2, sm + L::sH2, r);
+        hidden_epilogue<!TRAIN>(lane_base + col_z2<MODE>(), b2, sm + L::sH2, r);
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
