@@ -69,10 +69,25 @@ struct Slab {
     static constexpr size_t smem() { return 2 * (size_t)(Q + 7) * BYTES + 64; }
 };
 
+// Threads 0 .. kPhiBorder - 1 each fill one element of the phi ring's
+// 2-cell border on every plane (the others fill only their own column).
+constexpr int kPhiBorder = kHX * kHY - kThreads; // 176
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;
+static_assert(kHX * kHY <= 1024, "a ring position fits the 10 bits BulkSmem::bpack gives it");
+
 struct BulkSmem {
     float phiZ[6][kHY][kHX]; // phi as computeForces sees it (ghost / outside read as 0)
     float nrm[3][4][kNY][kNX]; // n_x, n_y, n_z, |grad phi| on the zeroed field
     float carry[11][kThreads]; // gradient and curvature carries, one column per thread
+    // the border element of thread tid, the same on every plane of a work
+    // item: its in-plane cell index (kNoCell where the element is a ghost or
+    // outside cell in x or y) and, packed, its position in a ring plane
+    // (hy * kHX + hx, bits 0-9) and which of its x-1, x+1, y-1, y+1
+    // neighbours wrap an exact-periodic axis (bits 10-13); 1 KB, so that four
+    // blocks (of the batched kernel too) stay within the 164 KB shared-memory
+    // carve-out and leave the L1 cache its 92 KB
+    uint32_t bcell[kPhiBorder];
+    uint16_t bpack[kPhiBorder];
 };
 
 // Ring slot of plane p; planes never go below -2, so the unsigned form is exact.
@@ -131,7 +146,6 @@ struct Bulk {
     // is filled one element per thread for the thread's own column and one
     // more for tid < kPhiBorder, which covers the border: rows 0-1 and 10-11,
     // then columns 0, 1, 34, 35 of rows 2-9.
-    static constexpr int kPhiBorder = kHX * kHY - kThreads; // 176
     static __device__ __forceinline__ void phi_border_pos(int tid, int &hx, int &hy) {
         if (tid < 2 * kHX) {
             hy = tid / kHX;
@@ -145,6 +159,43 @@ struct Bulk {
             hy = 2 + (k >> 2);
             hx = c < 2 ? c : kHX - 4 + c;
         }
+    }
+
+    // Thread tid's border element, once per work item (BulkSmem::bcell, bpack).
+    static __device__ void border_setup(const A &a, BulkSmem &S, int x0, int y0, int tid) {
+        const Geometry &G = a.geo;
+        int hx, hy;
+        phi_border_pos(tid, hx, hy);
+        const int bx = halo_axis(a, x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
+        const int by = halo_axis(a, y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
+        const bool fl = bx >= G.x_lo && bx <= G.x_hi && by >= G.y_lo && by <= G.y_hi;
+        S.bcell[tid] = fl ? (uint32_t)bx + G.nx * (uint32_t)by : kNoCell;
+        S.bpack[tid] = (uint16_t)((hy * kHX + hx) | (bx == 0 ? 1 << 10 : 0) | (bx == (int)G.nx - 1 ? 1 << 11 : 0) |
+                                  (by == 0 ? 1 << 12 : 0) | (by == (int)G.ny - 1 ? 1 << 13 : 0));
+    }
+
+    // The 7 phase populations of fluid cell c (lattice index) whose in-plane
+    // neighbours wrap as `wrap` says (bits 10-13 of BulkSmem::bpack), on plane
+    // gz: the gathers of phi_from_g.
+    static __device__ __forceinline__ void border_gather(const A &a, uint32_t c, uint32_t wrap, int gz,
+                                                         float (&g)[7]) {
+        const Geometry &G = a.geo;
+        const uint32_t xm = c + ((wrap & (1u << 10)) ? G.nx - 1 : (uint32_t)-1);
+        const uint32_t xp = c + ((wrap & (1u << 11)) ? (uint32_t)(1 - (int)G.nx) : 1u);
+        const uint32_t ym = c + ((wrap & (1u << 12)) ? G.nxy - G.nx : (uint32_t)-(int)G.nx);
+        const uint32_t yp = c + ((wrap & (1u << 13)) ? (uint32_t)-(int)(G.nxy - G.nx) : G.nx);
+        const uint32_t zm = c + (gz == 0 ? (uint32_t)(G.cells - G.nxy) : (uint32_t)-(int)G.nxy);
+        const uint32_t zp = c + (gz == (int)G.nz - 1 ? (uint32_t)-(int64_t)(G.cells - G.nxy) : G.nxy);
+        g[0] = Store<TG>::ld_keep(a.gq_src[0] + c);
+        g[1] = Store<TG>::ld_keep(a.gq_src[1] + xm);
+        g[2] = Store<TG>::ld_keep(a.gq_src[2] + xp);
+        g[3] = Store<TG>::ld_keep(a.gq_src[3] + ym);
+        g[4] = Store<TG>::ld_keep(a.gq_src[4] + yp);
+        g[5] = Store<TG>::ld_keep(a.gq_src[5] + zm);
+        g[6] = Store<TG>::ld_keep(a.gq_src[6] + zp);
+    }
+    static __device__ __forceinline__ float sum7(const float (&g)[7]) {
+        return (((((g[0] + g[1]) + g[2]) + g[3]) + g[4]) + g[5]) + g[6];
     }
 
     // Fill ring slot of plane pz with phi over the tile + 2-cell halo: fluid
@@ -245,6 +296,7 @@ struct Bulk {
         const int x = x0 + tx, y = y0 + ty;
         const bool active = x >= G.x_lo && x <= G.x_hi && y >= G.y_lo && y <= G.y_hi;
         for (int p = zs - 2; p <= zs + 3; ++p) fill_phi(a, S, x0, y0, p, tid);
+        if (tid < kPhiBorder) border_setup(a, S, x0, y0, tid); // read back by this thread only
         __syncthreads();
         GradCarry gc(S, tid);
         gc.start(S.phiZ[ringP(zs - 2)], S.phiZ[ringP(zs - 1)], tx + 2, ty + 2);
@@ -274,16 +326,17 @@ struct Bulk {
                 if (z + 2 <= ze) fill_nrm_carry(S, z + 2, tid, gc);
                 if (more) {
                     const int sp = ringP(z + 4);
-                    S.phiZ[sp][ty + 2][tx + 2] = (((((go[0] + go[1]) + go[2]) + go[3]) + go[4]) + go[5]) + go[6];
+                    S.phiZ[sp][ty + 2][tx + 2] = sum7(go);
                     if (tid < kPhiBorder) {
-                        int hx, hy;
-                        phi_border_pos(tid, hx, hy);
-                        const int bx = halo_axis(a, x0 - 2 + hx, G.nx, G.bcx == BC_PERIODIC);
-                        const int by = halo_axis(a, y0 - 2 + hy, G.ny, G.bcy == BC_PERIODIC);
+                        // the border element: its cell and wraps from border_setup
+                        const uint32_t c = S.bcell[tid], pk = S.bpack[tid];
                         float v = 0.f;
-                        if (zf && bx >= G.x_lo && bx <= G.x_hi && by >= G.y_lo && by <= G.y_hi)
-                            v = phi_from_g(a, bx, by, gz, cell_index(G, bx, by, gz));
-                        S.phiZ[sp][hy][hx] = v;
+                        if (zf && c != kNoCell) {
+                            float gb[7];
+                            border_gather(a, c + (uint32_t)gz * G.nxy, pk, gz, gb);
+                            v = sum7(gb);
+                        }
+                        (&S.phiZ[sp][0][0])[pk & 0x3FFu] = v;
                     }
                 }
             }
