@@ -730,7 +730,8 @@ def run_ours(a, world, rank, local):
     # weigh K / JOB_STEPS times more
     e2e_steps = max(JOB_STEPS, a.steps)
     barrier(world)
-    e2e_local, h2d, d2h = e2e_run(p, e2e_steps)
+    with ClockSampler(local) as clk_e2e:
+        e2e_local, h2d, d2h = e2e_run(p, e2e_steps)
     barrier(world)
     e2e_k_local, h2d_k, d2h_k = e2e_run(p, max(a.steps, 2))
     # every replica ran the same job: the slowest one sets the time
@@ -770,7 +771,8 @@ def run_ours(a, world, rank, local):
                 "job": f"the jet's configured run: {e2e_steps} steps from the initial state uploaded "
                        "from pinned host memory to the download of phi and rho, through the C ABI",
                 "k_steps": {"value": round(e2e_k_mlups, 1), "steps": max(a.steps, 2),
-                            "h2d_bytes_per_step": int(h2d_k), "d2h_bytes_per_step": int(d2h_k)}},
+                            "h2d_bytes_per_step": int(h2d_k), "d2h_bytes_per_step": int(d2h_k)},
+                "clocks": clk_e2e.summary()},
         "gpu_launches": a.steps * (1 + n_bc),
         "clocks": clocks,
         "variants": variants,

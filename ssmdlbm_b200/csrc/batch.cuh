@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kThreads, kBulkMinBlocks<Q>)
         const int bz = w / sa.tiles_y;
         const int zs = sa.geo.z_lo + bz * sa.zchunk;
         const int ze = min(zs + sa.zchunk, sa.geo.z_hi + 1);
-        B::run_gather(sa, S, bx * kTX, by * kTY, zs, ze, tx, ty, tid);
+        B::template run_gather<false>(sa, S, bx * kTX, by * kTY, zs, ze, tx, ty, tid);
     }
 }
 
