@@ -313,7 +313,7 @@ struct Bulk {
         for (int z = zs; z < ze; ++z) {
             // the plane terms after the population gathers are issued
             // (D3Q19 with FP32 storage: before them, measured faster on B200)
-            constexpr bool kEarly = Q == 19 && std::is_same<TF, float>::value;
+            constexpr bool kEarly = Q == 19;
             if (active) cell_lazy<kEarly>(a, S, x, y, z, tx, ty, [&] { return cv.advance(S, z, tx, ty); });
             else cv.advance(S, z, tx, ty);
             {
