@@ -311,8 +311,8 @@ struct Bulk {
         cv.start(S, zs, tx, ty);
         __syncthreads();
         for (int z = zs; z < ze; ++z) {
-            // the plane terms after the population gathers are issued
-            // (D3Q19 with FP32 storage: before them, measured faster on B200)
+            // the plane terms after the population gathers are issued (D3Q19:
+            // before them, measured faster on B200 for FP32 and 16-bit storage)
             constexpr bool kEarly = Q == 19;
             if (active) cell_lazy<kEarly>(a, S, x, y, z, tx, ty, [&] { return cv.advance(S, z, tx, ty); });
             else cv.advance(S, z, tx, ty);
