@@ -31,10 +31,13 @@
 // dH2 = dR W3 and dZ2 = dH2 gelu'(z2 + b2) on the CUDA cores (N = 2 is too
 // narrow for an MMA), dH1 = dZ2 W2 on the tensor cores, dZ1 = dH1 gelu'(z1 +
 // b1); the weight and bias gradients (sums over a tile's 128 rows) on the
-// CUDA cores in FP32, carried in registers across the CTA's tiles, then
-// either added across CTAs with atomics (ssmd_mlp_grad) or written as one row
-// per CTA and summed in CTA order by a second kernel (ssmd_mlp_grad_ws:
-// the same bits on every run).  Every wait on an MMA is bounded: on timeout
+// tensor cores too: the epilogues also write H1, H2, X, dZ1, dZ2 and dR
+// transposed (bf16, K = the tile's rows), and two MMAs per tile accumulate
+// dW2^T, dW3^T (G1) and dW1^T with the bias gradients (G2, through a row of
+// ones) in TMEM across the CTA's tiles; they run while the next tile's
+// features load.  The CTA's sums are then either added across CTAs with
+// atomics (ssmd_mlp_grad) or written as one row per CTA and summed in CTA
+// order by a second kernel (ssmd_mlp_grad_ws: the same bits on every run).  Every wait on an MMA is bounded: on timeout
 // the CTA records bit 0 of the status word, frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -62,24 +65,36 @@ static_assert(kNet == SSMD_MLP_NET_FLOATS, "network layout");
 enum : int { kFwd = 0, kTrain = 1, kRefresh = 2 };
 
 // TMEM columns: training keeps z1 (0-63) and z2 (64-127) for the backward
-// pass, r at 128-143 and dH1 at 192-255; inference puts z1, z2 and r in turn
-// on columns 0-63.
+// pass, r at 128-143, dH1 at 192-255 and the CTA's weight-gradient sums
+// across its tiles at 256-335 (G1) and 336-479 (G2); inference puts z1, z2
+// and r in turn on columns 0-63.
 template <int MODE>
-constexpr uint32_t tmem_cols() { return MODE == kTrain ? 256u : 64u; }
+constexpr uint32_t tmem_cols() { return MODE == kTrain ? 512u : 64u; }
 template <int MODE>
 constexpr uint32_t col_z2() { return MODE == kTrain ? 64u : 0u; }
 template <int MODE>
 constexpr uint32_t col_r() { return MODE == kTrain ? 128u : 0u; }
-constexpr uint32_t cZ1 = 0, cDH1 = 192;
+constexpr uint32_t cZ1 = 0, cDH1 = 192, cG1 = 256, cG2 = 336;
+constexpr int kGK = kRows;         // K of the weight-gradient MMAs: the tile's rows
+constexpr int kGB = 2 * kH + 16;   // rows of the gradient B tile: dZ1^T, dZ2^T, dR^T (2 of 16)
 constexpr uint64_t kMmaWaitNs = 1000000000ull;
-constexpr int kLd = 65; // fp32 row stride of the dZ staging arrays (bank-conflict free)
 constexpr int kMaxGradCtas = 256; // rows of the deterministic gradient workspace
 
 // shared-memory map (bytes from an aligned base: 1024 bytes for training,
-// 128 for inference; the no-swizzle operand layout needs 16); training-only tiles:
-// W2^T, bf16 dZ2, FP32 dZ2 and dZ1 staging, dL/dr
-constexpr uint32_t sW2T = 49152, sDZ2 = 57344, sDZ2F = 73728, sDZ1F = sDZ2F + kRows * kLd * 4,
-                   sDY = sDZ1F + kRows * kLd * 4;
+// 128 for inference; the no-swizzle operand layout needs 16); training-only
+// tiles: W2^T, bf16 dZ2, and the operands of the weight-gradient MMAs, all
+// K-major with K = the tile's 128 rows:
+//   GA2 [16 x 128]: X^T (rows 0-11), a row of ones (12), zeros (13-15); the
+//       M = 128 MMA reads rows 16-127 from GA1 that follows (their products
+//       land in accumulator rows nobody reads)
+//   GA1 [128 x 128]: H1^T (rows 0-63), H2^T (rows 64-127)
+//   GB  [144 x 128]: dZ1^T (rows 0-63), dZ2^T (64-127), dR^T (128-129), zeros
+// so that G1 = GA1 GB[64..143]^T holds dW2^T and dW3^T, and G2 = GA2 GB^T
+// holds dW1^T and, in its ones row, the three bias gradients; then a small
+// scratch for the per-warp losses
+constexpr uint32_t sW2T = 49152, sDZ2 = 57344, sGA2 = 73728, sGA1 = sGA2 + 16 * kGK * 2,
+                   sGB = sGA1 + kRows * kGK * 2, sDY = sGB + kGB * kGK * 2;
+static_assert(sGA2 + (uint32_t)kRows * kGK * 2 <= sGB, "the M = 128 read of GA2 stays inside GA2 + GA1");
 template <int MODE>
 struct Layout {
     static constexpr bool T = MODE == kTrain;
@@ -157,9 +172,6 @@ __device__ __forceinline__ void st8(unsigned char *tile, int r, int k0, int K, c
     *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(r, k0, K)) = u;
 }
 
-__device__ __forceinline__ float ldbf(const unsigned char *tile, int r, int k, int K) {
-    return __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(tile + umma::kmajor_offset(r, k, K)));
-}
 
 // Copy a [rows x K] block of fp32 weights (row stride K), times `scale` (a
 // power of two), into a bf16 tile of rows_pad rows (extra rows zero);
@@ -183,12 +195,24 @@ __device__ __forceinline__ bool wait_mma(uint64_t *bar, uint32_t phase, volatile
     return ok;
 }
 
+// Element (m, k) of a K-major bf16 tile with K = kGK (the weight-gradient
+// operands: the tile's rows r are their K).
+__device__ __forceinline__ void st_g(unsigned char *tile, int m, int k, uint16_t bits) {
+    *reinterpret_cast<uint16_t *>(tile + umma::kmajor_offset(m, k, kGK)) = bits;
+}
+__device__ __forceinline__ uint16_t bf16_bits(float v) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    return *reinterpret_cast<const uint16_t *>(&h);
+}
+
 // Bias + GELU epilogue of a 64-column accumulator into a [128 x 64] bf16 tile
-// (TWICE: 2 gelu, for a next layer staged with halved weights).  The TMEM
-// load of columns 16 (c + 1) .. 16 c + 31 is in flight while columns 16 c ..
-// 16 c + 15 are processed.
-template <bool TWICE = false>
-__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bias, unsigned char *tile, int r) {
+// (TWICE: 2 gelu, for a next layer staged with halved weights; TRANS: the
+// same bf16 values also into column r, rows trow0 .. trow0 + 63, of a
+// weight-gradient operand tile).  The TMEM load of columns 16 (c + 1) ..
+// 16 c + 31 is in flight while columns 16 c .. 16 c + 15 are processed.
+template <bool TWICE = false, bool TRANS = false>
+__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bias, unsigned char *tile, int r,
+                                                unsigned char *ttile = nullptr, int trow0 = 0) {
     uint32_t nxt[16];
     umma::tmem_ld16_issue(taddr, nxt);
 #pragma unroll
@@ -206,6 +230,13 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float *bia
             const float2 g1 = gelu2<TWICE>(__fadd2_rn(make_float2(v[4 * i + 2], v[4 * i + 3]), make_float2(b.z, b.w)));
             pk[2 * i] = pack2(g0.x, g0.y);
             pk[2 * i + 1] = pack2(g1.x, g1.y);
+        }
+        if constexpr (TRANS) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                st_g(ttile, trow0 + 16 * c + 2 * i, r, (uint16_t)(pk[i] & 0xFFFFu));
+                st_g(ttile, trow0 + 16 * c + 2 * i + 1, r, (uint16_t)(pk[i] >> 16));
+            }
         }
         *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(r, 16 * c, kH)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(r, 16 * c + 8, kH)) =
@@ -283,20 +314,25 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
         for (int e = tid; e < kOut * kH; e += kThreadsMlp) w3f[e] = net[oW3 + e];
     if (tid < kOut) b3[tid] = net[oB3 + tid];
     if (tid < kNet - kParams) norm[tid] = net[kParams + tid];
+    if constexpr (TRAIN) {
+        // the rows of the gradient operands that no tile writes: GA2 row 12
+        // all ones (its products are the column sums, the bias gradients),
+        // rows 13-15 and GB rows 130-143 zero
+        const uint16_t one = bf16_bits(1.0f);
+        st_g(sm + sGA2, 12, tid, one);
+        for (int m = 13; m < 16; ++m) st_g(sm + sGA2, m, tid, 0);
+        for (int m = 2 * kH + kOut; m < kGB; ++m) st_g(sm + sGB, m, tid, 0);
+    }
     __syncthreads();
 
     const int r = tid;
     const uint32_t sbase = smem_addr(sm);
     uint32_t phase = 0;
     bool ok = true;
-    // weight-gradient partial sums of this CTA, carried across its tiles
-    float gw2[32], gw1[8], gw3 = 0.f, gb = 0.f, gb3 = 0.f;
-    if constexpr (TRAIN) {
-#pragma unroll
-        for (int i = 0; i < 32; ++i) gw2[i] = 0.f;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) gw1[i] = 0.f;
-    }
+    // training: the weight-gradient MMAs of a tile run while the next tile's
+    // features load; gpend says they are in flight (waited for before the
+    // next tile writes their operands, and after the last tile)
+    bool gpend = false, gfirst = true;
     float lsum = 0.f;
     const int64_t tiles = (n + kRows - 1) / kRows;
     uint32_t tmem = 0, lane_base = 0;
@@ -310,6 +346,16 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
             load_row<MODE>(a, norm, row, valid, x, nu_phi);
             st8(sm + L::sX, r, 0, kK1, x);
             st8(sm + L::sX, r, 8, kK1, x + 8);
+            if constexpr (TRAIN) {
+                if (gpend) { // the previous tile's gradient MMAs read GA2, GA1, GB
+                    ok = wait_mma(bar, phase, abort_flag);
+                    phase ^= 1u;
+                    gpend = false;
+                    if (!ok) break;
+                }
+#pragma unroll
+                for (int k = 0; k < kIn; ++k) st_g(sm + sGA2, k, r, bf16_bits(x[k])); // X^T
+            }
         }
         fence_proxy_async(); // generic-proxy smem writes -> visible to the tensor core
         umma::fence_before_sync();
@@ -327,7 +373,7 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue<!TRAIN>(lane_base + cZ1, b1, sm + L::sH1, r);
+        hidden_epilogue<!TRAIN, TRAIN>(lane_base + cZ1, b1, sm + L::sH1, r, sm + sGA1, 0); // (H1^T)
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
@@ -344,7 +390,7 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
         ok = wait_mma(bar, phase, abort_flag);
         phase ^= 1u;
         if (!ok) break;
-        hidden_epilogue<!TRAIN>(lane_base + col_z2<MODE>(), b2, sm + L::sH2, r);
+        hidden_epilogue<!TRAIN, TRAIN>(lane_base + col_z2<MODE>(), b2, sm + L::sH2, r, sm + sGA1, kH); // (H2^T)
         fence_proxy_async();
         umma::fence_before_sync();
         __syncthreads();
@@ -383,9 +429,6 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
                 a.cs[row] = fminf(fmaxf(p1, 0.25f), 4.0f);
             }
         } else {
-            float *dzf2 = reinterpret_cast<float *>(sm + sDZ2F);
-            float *dzf1 = reinterpret_cast<float *>(sm + sDZ1F);
-            float *dy = reinterpret_cast<float *>(sm + sDY);
             // ---- loss and dL/dr
             float d0 = 0.f, d1 = 0.f;
             if (valid) {
@@ -399,8 +442,8 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
                 d0 = 2.0f * w0 * e0 * inv_n;
                 d1 = 2.0f * w1 * e1 * inv_n;
             }
-            dy[r * kOut + 0] = d0;
-            dy[r * kOut + 1] = d1;
+            st_g(sm + sGB, 2 * kH + 0, r, bf16_bits(d0)); // dR^T
+            st_g(sm + sGB, 2 * kH + 1, r, bf16_bits(d1));
             // ---- dZ2 = (dR W3) * gelu'(z2 + b2)
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -411,7 +454,7 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
                     const int j = 16 * c + i;
                     const float dh = fmaf(d0, w3f[j], d1 * w3f[kH + j]);
                     v[i] = dh * gelu_grad(v[i] + b2[j]);
-                    dzf2[r * kLd + j] = v[i];
+                    st_g(sm + sGB, kH + j, r, bf16_bits(v[i])); // dZ2^T
                 }
                 st8(sm + sDZ2, r, 16 * c, kH, v);
                 st8(sm + sDZ2, r, 16 * c + 8, kH, v + 8);
@@ -437,52 +480,36 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
                 umma::tmem_ld16(lane_base + cDH1 + 16 * c, dh);
                 umma::tmem_ld16(lane_base + cZ1 + 16 * c, z);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) dzf1[r * kLd + 16 * c + i] = dh[i] * gelu_grad(z[i] + b1[16 * c + i]);
+                for (int i = 0; i < 16; ++i)
+                    st_g(sm + sGB, 16 * c + i, r, bf16_bits(dh[i] * gelu_grad(z[i] + b1[16 * c + i]))); // dZ1^T
             }
+            fence_proxy_async();
+            umma::fence_before_sync();
             __syncthreads();
-            // ---- weight and bias gradients of this tile: sums over its 128 rows
-            {   // dW2[o][i] = sum_r dZ2[r][o] H1[r][i]: thread -> (o, 32 i)
-                const int o = tid >> 1, i0 = (tid & 1) * 32;
-                for (int rr2 = 0; rr2 < kRows; ++rr2) {
-                    const float d = dzf2[rr2 * kLd + o];
-#pragma unroll
-                    for (int ch = 0; ch < 4; ++ch) {
-                        const uint4 u = *reinterpret_cast<const uint4 *>(sm + L::sH1 +
-                                                                         umma::kmajor_offset(rr2, i0 + 8 * ch, kH));
-                        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const float2 f2 = __bfloat1622float2(h[e]);
-                            gw2[8 * ch + 2 * e] = fmaf(d, f2.x, gw2[8 * ch + 2 * e]);
-                            gw2[8 * ch + 2 * e + 1] = fmaf(d, f2.y, gw2[8 * ch + 2 * e + 1]);
-                        }
-                    }
-                }
+            // ---- weight and bias gradients of this tile, summed over its 128
+            // rows (the MMAs' K) into the CTA's accumulators G1 and G2:
+            //   G1 [128 x 80]  += GA1 GB[64..143]^T: rows 0-63 dW2^T, rows 64-127 cols 64-65 dW3^T
+            //   G2 [128 x 144] += GA2 GB^T: rows 0-11 cols 0-63 dW1^T; row 12: db1, db2, db3
+            if (tid == 0) {
+                umma::fence_after_sync();
+                for (int ks = 0; ks < kGK / 16; ++ks)
+                    umma::mma_bf16(tmem + cG1, umma::smem_desc(sbase + sGA1 + 256 * ks, 128, 2048),
+                                   umma::smem_desc(sbase + sGB + (kH / 8) * 2048 + 256 * ks, 128, 2048),
+                                   umma::idesc_bf16(128, kGB - kH), !gfirst || ks > 0);
+                for (int ks = 0; ks < kGK / 16; ++ks)
+                    umma::mma_bf16(tmem + cG2, umma::smem_desc(sbase + sGA2 + 256 * ks, 128, 2048),
+                                   umma::smem_desc(sbase + sGB + 256 * ks, 128, 2048), umma::idesc_bf16(128, kGB),
+                                   !gfirst || ks > 0);
+                umma::commit(bar);
             }
-            {   // dW1[o][i] = sum_r dZ1[r][o] X[r][i]: thread -> (o, 8 i)
-                const int o = tid >> 1, i0 = (tid & 1) * 8;
-                for (int rr2 = 0; rr2 < kRows; ++rr2) {
-                    const float d = dzf1[rr2 * kLd + o];
-                    const uint4 u = *reinterpret_cast<const uint4 *>(sm + L::sX + umma::kmajor_offset(rr2, i0, kK1));
-                    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float2 f2 = __bfloat1622float2(h[e]);
-                        gw1[2 * e] = fmaf(d, f2.x, gw1[2 * e]);
-                        gw1[2 * e + 1] = fmaf(d, f2.y, gw1[2 * e + 1]);
-                    }
-                }
-            }
-            {   // dW3[k][j] = sum_r dR[r][k] H2[r][j]; db2 (k = 0 threads), db1 (k = 1); db3
-                const int k = tid >> 6, j = tid & 63;
-                for (int rr2 = 0; rr2 < kRows; ++rr2) {
-                    gw3 = fmaf(dy[rr2 * kOut + k], ldbf(sm + L::sH2, rr2, j, kH), gw3);
-                    gb += k == 0 ? dzf2[rr2 * kLd + j] : dzf1[rr2 * kLd + j];
-                }
-                if (tid < kOut)
-                    for (int rr2 = 0; rr2 < kRows; ++rr2) gb3 += dy[rr2 * kOut + tid];
-            }
-            __syncthreads(); // the next tile overwrites X, H1, H2 and the dZ staging
+            gpend = true;
+            gfirst = false;
+        }
+    }
+    if constexpr (TRAIN) {
+        if (ok && gpend) {
+            ok = wait_mma(bar, phase, abort_flag);
+            phase ^= 1u;
         }
     }
 
@@ -494,16 +521,41 @@ __global__ void __launch_bounds__(kThreadsMlp, MODE == kTrain ? 1 : 7) mlp_kerne
                 if (a.partials) dst[k] = v;
                 else atomicAdd(&dst[k], v);
             };
-            const int o = tid >> 1;
-            const int i0 = (tid & 1) * 32, i1 = (tid & 1) * 8;
+            // thread m reads row m of the accumulators (warp w holds lanes 32 w ..)
+            const int m = tid;
+            if (!gfirst) {
+                const uint32_t lb = *slot + ((uint32_t)(warp * 32) << 16);
+                float v[16];
+                if (m < kH) { // dW2[o][m] = G1[m][o]
 #pragma unroll
-            for (int i = 0; i < 32; ++i) put(oW2 + o * kH + i0 + i, gw2[i]);
+                    for (int c = 0; c < kH / 16; ++c) {
+                        umma::tmem_ld16(lb + cG1 + 16 * c, v);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) put(oW1 + o * kK1 + i1 + i, i1 + i < kIn ? gw1[i] : 0.f);
-            const int k = tid >> 6, j = tid & 63;
-            put(oW3 + k * kH + j, gw3);
-            put((k == 0 ? oB2 : oB1) + j, gb);
-            if (tid < kOut) put(oB3 + tid, gb3);
+                        for (int i = 0; i < 16; ++i) put(oW2 + (16 * c + i) * kH + m, v[i]);
+                    }
+                } else { // dW3[k][m - 64] = G1[m][64 + k]
+                    umma::tmem_ld16(lb + cG1 + kH, v);
+                    put(oW3 + 0 * kH + (m - kH), v[0]);
+                    put(oW3 + 1 * kH + (m - kH), v[1]);
+                }
+                if (warp == 0) { // warp-collective loads: lanes 0-11 dW1, lane 12 the biases
+                    for (int c = 0; c < kGB / 16; ++c) {
+                        umma::tmem_ld16(lb + cG2 + 16 * c, v);
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const int col = 16 * c + i;
+                            if (col < kH && m < kK1) put(oW1 + col * kK1 + m, m < kIn ? v[i] : 0.f); // dW1[o][m]
+                            if (m == kIn) {
+                                if (col < kH) put(oB1 + col, v[i]);
+                                else if (col < 2 * kH) put(oB2 + col - kH, v[i]);
+                                else if (col < 2 * kH + kOut) put(oB3 + col - 2 * kH, v[i]);
+                            }
+                        }
+                    }
+                }
+            } else { // a CTA without tiles adds zeros
+                for (int e = tid; e < kParams; e += kThreadsMlp) put(e, 0.f);
+            }
             float l = lsum;
             for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
             if (a.partials) {
