@@ -609,7 +609,7 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
     }
 
 
-def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000):
+def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000, average: float | None = None):
     """The closure study's data generation and training: fine D3Q19 jets
     256 x 256 x 1024 (nozzle 32, tau 0.55, sigma 1e-3, M 0.1, 1 % noise),
     inlet w ~ U[0.04, 0.08] per seed, `steps` steps each, filtered 2x onto
@@ -642,7 +642,8 @@ def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000):
     net.normalise(feats, tg)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    curve = net.train(feats, tg, wt, train_steps, 65536, 1e-3, 0, report_every=max(1, train_steps // 10))
+    curve = net.train(feats, tg, wt, train_steps, 65536, 1e-3, 0, report_every=max(1, train_steps // 10),
+                      average=average)
     e1.record()
     e1.synchronize()
     per_seed = []

@@ -462,6 +462,9 @@ int ssmd_derived_update(const ssmd_params *p, const LBMFields *fields, uint32_t 
  *     sums to a row of `workspace` (ssmd_mlp_grad_workspace_bytes() bytes,
  *     device memory) and a second kernel adds the rows in CTA order.
  *   ssmd_mlp_adam: one Adam step (bias-corrected, step t >= 1) on the params.
+ *   ssmd_mlp_average: avg = decay * avg + (1 - decay) * net on the params (an
+ *     exponential moving average of the weights along training; the
+ *     normalisation part of avg is left as it is).
  *   ssmd_mlp_status: bit 0 set when an MMA wait timed out (the CTA aborted).
  * Features (ssmd_closure_features), per cell, from rho, ux, uy, uz, phi with
  * central differences (periodic axes wrap, others clamp at the faces):
@@ -493,6 +496,7 @@ int ssmd_mlp_grad_ws(const float *net, const float *features, const float *targe
                      ssmd_stream_t stream);
 int ssmd_mlp_adam(float *net, const float *grad, float *m, float *v, int64_t t, float lr, float beta1,
                   float beta2, float eps, ssmd_stream_t stream);
+int ssmd_mlp_average(float *avg, const float *net, float decay, ssmd_stream_t stream);
 int ssmd_mlp_status(uint32_t *status);
 int ssmd_closure_features(const ssmd_params *p, const LBMFields *fields, float *features, ssmd_stream_t stream);
 int ssmd_closure_filter(const ssmd_params *fine, const LBMFields *fine_fields, float *coarse, float *tau,

@@ -169,6 +169,7 @@ SIGNATURES = [
                                    c_void_p, ctypes.c_size_t, c_void_p]),
     ("ssmd_mlp_adam", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64, c_float, c_float,
                                 c_float, c_float, c_void_p]),
+    ("ssmd_mlp_average", c_int32, [c_void_p, c_void_p, c_float, c_void_p]),
     ("ssmd_mlp_status", c_int32, [POINTER(c_uint32)]),
     ("ssmd_closure_features", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_void_p]),
     ("ssmd_closure_filter", c_int32, [POINTER(Params), POINTER(LBMFields), c_void_p, c_void_p, c_void_p,

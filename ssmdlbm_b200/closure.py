@@ -117,9 +117,13 @@ class Network:
         return float(self.loss.item())
 
     def train(self, feats, targets, weights, steps: int, batch: int = 65536, lr: float = 1e-3, seed: int = 0,
-              report_every: int = 0) -> list:
-        """Adam on random mini-batches (rows drawn with replacement)."""
+              report_every: int = 0, average: float | None = None) -> list:
+        """Adam on random mini-batches (rows drawn with replacement).  With
+        `average` (a decay in (0, 1)) the network ends on the exponential
+        moving average of its weights along the run (ssmd_mlp_average after
+        every step) instead of the last step's weights."""
         L = lib()
+        avg = self.net.clone() if average is not None else None
         st = torch.cuda.current_stream(self.device).cuda_stream
         gen = torch.Generator(device=self.device)
         gen.manual_seed(seed)
@@ -138,8 +142,13 @@ class Network:
             self.t += 1
             check(L.ssmd_mlp_adam(self.net.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(), self.v.data_ptr(),
                                   self.t, lr, 0.9, 0.999, 1e-8, st))
+            if avg is not None:
+                check(L.ssmd_mlp_average(avg.data_ptr(), self.net.data_ptr(), average, st))
             if report_every and (k % report_every == 0 or k == steps - 1):
                 losses.append((k, float(self.loss.item())))
+        if avg is not None:
+            P = _lib.MLP_PARAMS
+            self.net[:P] = avg[:P]
         return losses
 
     def predict(self, feats: torch.Tensor) -> torch.Tensor:
@@ -367,7 +376,7 @@ def stat_errors(s: JetStats, ref: JetStats) -> dict:
 
 def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train_steps: int = 2000,
                batch: int = 65536, lr: float = 1e-3, seed: int = 0, update_every: int = 1,
-               nut_max: float = 0.05, coarse_storage: int | None = None) -> dict:
+               nut_max: float = 0.05, coarse_storage: int | None = None, average: float | None = None) -> dict:
     """Fine run (the judge and the data), training, then the coarse lattice
     plain and with the trained closure (population storage `coarse_storage`,
     default the fine run's); statistics, errors and device times."""
@@ -394,7 +403,8 @@ def experiment(fine_p: Params, steps: int, sample_every: int, spinup: int, train
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     curve = net.train(f_tr if f_tr.shape[0] else feats, t_tr if f_tr.shape[0] else tg,
-                      w_tr if f_tr.shape[0] else wt, train_steps, batch, lr, seed, report_every=max(1, train_steps // 10))
+                      w_tr if f_tr.shape[0] else wt, train_steps, batch, lr, seed,
+                      report_every=max(1, train_steps // 10), average=average)
     e1.record()
     e1.synchronize()
     train_s = e0.elapsed_time(e1) / 1e3

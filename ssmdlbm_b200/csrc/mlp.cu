@@ -607,6 +607,12 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
     p[i] -= lr * (mi / corr1) / (sqrtf(vi / corr2) + eps);
 }
 
+__global__ void average_kernel(float *__restrict__ avg, const float *__restrict__ p, int count, float decay) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    avg[i] = fmaf(decay, avg[i] - p[i], p[i]); // decay avg + (1 - decay) p
+}
+
 // Resident CTAs per SM of a mode and the SM count, computed once per mode and
 // device from the device's limits: shared memory (with the per-block
 // reservation), registers (allocated per warp in multiples of 8 per thread),
@@ -764,6 +770,14 @@ extern "C" int ssmd_mlp_adam(float *net, const float *grad, float *m, float *v, 
     adam_kernel<<<(kParams + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         net, grad, m, v, kParams, lr, beta1, beta2, eps, corr1, corr2);
     return cuda_check(cudaGetLastError(), "adam launch");
+}
+
+extern "C" int ssmd_mlp_average(float *avg, const float *net, float decay, ssmd_stream_t stream) {
+    if (!avg || !net || !(decay >= 0.0f && decay <= 1.0f))
+        return fail(SSMD_ERR_INVALID_ARGUMENT, "null argument or decay outside [0, 1]");
+    average_kernel<<<(kParams + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(avg, net, kParams,
+                                                                                              decay);
+    return cuda_check(cudaGetLastError(), "average launch");
 }
 
 extern "C" int ssmd_mlp_status(uint32_t *status) {

@@ -137,6 +137,22 @@ def test_adam_matches_oracle():
     assert np.array_equal(dn.cpu().numpy()[co.PARAMS:], net[co.PARAMS:])
 
 
+def test_weight_average():
+    # avg <- decay avg + (1 - decay) net on the parameters; the normalisation
+    # part of avg stays as it was
+    rng = np.random.default_rng(5)
+    net, avg = _net(4), _net(5)
+    avg[co.PARAMS:] = rng.normal(0, 1, avg.size - co.PARAMS).astype(np.float32)
+    dn, da = _dev(net), _dev(avg)
+    check(lib().ssmd_mlp_average(da.data_ptr(), dn.data_ptr(), 0.99, None))
+    torch.cuda.synchronize()
+    ref = 0.99 * avg[:co.PARAMS].astype(np.float64) + 0.01 * net[:co.PARAMS].astype(np.float64)
+    got = da.cpu().numpy()
+    assert np.allclose(got[:co.PARAMS], ref, rtol=1e-6, atol=1e-7)
+    assert np.array_equal(got[co.PARAMS:], avg[co.PARAMS:])
+    assert lib().ssmd_mlp_average(da.data_ptr(), dn.data_ptr(), 1.5, None) == _lib.SSMD_ERR_INVALID_ARGUMENT
+
+
 def test_training_reduces_loss():
     rng = np.random.default_rng(4)
     n = 4096
