@@ -235,6 +235,16 @@ STORAGE_NAMES = {"f32": 0, "f16": 1, "bf16": 2, "f16g32": 3}
 # run length of the 128 x 128 x 512 jet as configured (the end-to-end leg runs it whole)
 JOB_STEPS = 5000
 
+# The closure network is kept as the exponential moving average of its
+# weights along training, decay 0.9999 (about the last 10 000 of its 20 000
+# Adam steps).  The networks the runs end on fit the held-out targets more
+# tightly but their effect on a coarse run changes sign from one training to
+# the next; the long average fits them less tightly and lowered the
+# centreline errors for four of five training seeds on the production jet
+# (where the decay was chosen) and on all eight jets of the closure study
+# (which played no part in the choice).
+CLOSURE_WEIGHT_AVERAGE = 0.9999
+
 # DRAM bytes per cell of one bulk launch on the 128 x 128 x 512 jet,
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of that
 # launch, keyed by (velocity set, storage): (bytes, the profiles/ summary
@@ -551,7 +561,7 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
     nut_max = 0.5 * float(fine_p.nu_water)
     r = closure.experiment(fine_p, steps=steps, sample_every=sample_every, spinup=spinup, train_steps=train_steps,
                            batch=65536, lr=1e-3, seed=0, update_every=update_every, nut_max=nut_max,
-                           coarse_storage=_lib.STORAGE_F16)
+                           coarse_storage=_lib.STORAGE_F16, average=CLOSURE_WEIGHT_AVERAGE)
     f, pl, cl = r["fine"], r["plain"], r["closure"]
     cp = closure.coarse_params(fine_p)
     cp.storage = _lib.STORAGE_F16
@@ -597,7 +607,8 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
         "coarse_closure": {"mlups": mlups(cl), "device_s": round(cl.device_s, 3), **bulk["coarse_f16"]},
         "nut_max": nut_max,
         "training": {"device_s": round(r["train_device_s"], 3), "adam_steps": train_steps, "samples": r["samples"],
-                     "heldout_loss": r["heldout_loss"], "reproducible_gradient": True},
+                     "heldout_loss": r["heldout_loss"], "reproducible_gradient": True,
+                     "weight_average_decay": CLOSURE_WEIGHT_AVERAGE},
         "time_ratio": round(cl.device_s / f.device_s, 4),
         "time_ratio_plain_coarse": round(pl.device_s / f.device_s, 4),
         "errors_vs_filtered_fine": {k: {"plain": r["errors_plain"][k], "closure": r["errors_closure"][k]}
@@ -609,7 +620,8 @@ def run_production(steps: int = 10000, sample_every: int = 1000, spinup: int = 5
     }
 
 
-def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000, average: float | None = None):
+def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000,
+           average: float | None = None):
     """The closure study's data generation and training: fine D3Q19 jets
     256 x 256 x 1024 (nozzle 32, tau 0.55, sigma 1e-3, M 0.1, 1 % noise),
     inlet w ~ U[0.04, 0.08] per seed, `steps` steps each, filtered 2x onto
@@ -643,7 +655,7 @@ def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000, average
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     curve = net.train(feats, tg, wt, train_steps, 65536, 1e-3, 0, report_every=max(1, train_steps // 10),
-                      average=average)
+                      average=CLOSURE_WEIGHT_AVERAGE if average is None else average)
     e1.record()
     e1.synchronize()
     per_seed = []
