@@ -292,8 +292,9 @@ struct Bulk {
     // Ends with a block-wide barrier.  BORDER_PRE: the phi ring's border
     // element from its sources found once per work item (border_setup);
     // otherwise found on every plane, which the batched kernel keeps (its
-    // extra live state spills more with the precompute: 18 947 against
-    // 19 684 MLUPS on the 48-lattice sweep).  Both give the same bits.
+    // extra live state spills more with the precompute: 18 872 against
+    // 19 590 MLUPS on the 48-lattice sweep, measured back to back).  Both
+    // give the same bits.
     template <bool BORDER_PRE = true>
     static __device__ void run_gather(const A &a, BulkSmem &S, int x0, int y0, int zs, int ze, int tx, int ty,
                                       int tid) {
