@@ -629,7 +629,9 @@ def run_c4(seeds: int = 8, steps: int = 20000, train_steps: int = 20000,
     each seed held out); one network trained on all seeds (Adam, lr 1e-3,
     batch 65536, `train_steps` steps, reproducible gradient); per seed, the
     held-out loss and the coarse run with and without the closure against
-    the filtered fine run."""
+    the filtered fine run.  `average`: decay of the moving average of the
+    weights the network is kept as (None: CLOSURE_WEIGHT_AVERAGE; 0: the last
+    step's weights)."""
     import numpy as np
     import torch
     from ssmdlbm_b200 import closure, configs
