@@ -12,7 +12,9 @@ results can be checked:
   emulated; the kernel's tanh is the SFU's tanh.approx.f32 (absolute error
   about 2^-11), so an activation near a bf16 rounding boundary may round the
   other way there;
-- its loss and gradient (the backward pass written out by hand) and Adam;
+- its loss and gradient (the backward pass written out by hand; the weight
+  and bias gradients take dZ1, dZ2 and dR rounded to bf16, the operands of
+  the kernel's gradient MMAs) and Adam;
 - features, 2x box filter and training targets, in FP32 arithmetic on
   [z][y][x] numpy arrays.
 """
@@ -117,15 +119,19 @@ def loss_and_grad(net, feat, target, weight=None, emulate_bf16: bool = True):
     dz2b = c["rb"](dz2.astype(np.float32)).astype(np.float64)
     dh1 = dz2b @ c["W2"]                          # tensor cores: bf16 dZ2, bf16 W2
     dz1 = dh1 * gelu_grad(c["z1"])
+    # the weight and bias gradients: sums over the rows of products of bf16
+    # operands (tensor cores; the bias sums through a row of ones)
+    dz1b = c["rb"](dz1.astype(np.float32)).astype(np.float64)
+    drb = c["rb"](dr.astype(np.float32)).astype(np.float64)
     g = np.zeros(PARAMS, np.float64)
-    gW1 = dz1.T @ c["x"]
+    gW1 = dz1b.T @ c["x"]
     gW1[:, IN:] = 0.0
     g[oW1:oB1] = gW1.reshape(-1)
-    g[oB1:oW2] = dz1.sum(0)
-    g[oW2:oB2] = (dz2.T @ c["h1"]).reshape(-1)
-    g[oB2:oW3] = dz2.sum(0)
-    g[oW3:oB3] = (dr.T @ c["h2"]).reshape(-1)
-    g[oB3:PARAMS] = dr.sum(0)
+    g[oB1:oW2] = dz1b.sum(0)
+    g[oW2:oB2] = (dz2b.T @ c["h1"]).reshape(-1)
+    g[oB2:oW3] = dz2b.sum(0)
+    g[oW3:oB3] = (drb.T @ c["h2"]).reshape(-1)
+    g[oB3:PARAMS] = drb.sum(0)
     return loss, g
 
 
